@@ -1,0 +1,391 @@
+// libbie_b200: C ABI, device-resident geometry, operator and solver
+// orchestration for the B200 layer-potential library. See include/bie_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/bie_b200.h"
+#include "host_setup.h"
+#include "solver.h"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+namespace bie {
+thread_local std::string g_last_error;
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(BIE_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void Buf::ensure(size_t need) {
+    if (need <= bytes) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = need + need / 4 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        throw Error(BIE_ENOMEM, "device allocation of " + std::to_string(want) + " bytes failed");
+    }
+    bytes = want;
+}
+void Buf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+}  // namespace bie
+
+using bie::Error;
+
+template <class F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return BIE_OK;
+    } catch (const Error& e) {
+        bie::g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        bie::g_last_error = "host allocation failed";
+        return BIE_ENOMEM;
+    } catch (const std::exception& e) {
+        bie::g_last_error = e.what();
+        return BIE_EINVAL;
+    } catch (...) {
+        bie::g_last_error = "unknown error";
+        return BIE_EINVAL;
+    }
+}
+
+#define REQUIRE(cond, msg) \
+    do {                   \
+        if (!(cond)) throw Error(BIE_EINVAL, msg); \
+    } while (0)
+
+struct bie_mesh {
+    bie::Mesh m;
+};
+struct bie_near {
+    bie::Near n;
+};
+
+extern "C" {
+
+int bie_last_error(char* buf, size_t len) {
+    const std::string& s = bie::g_last_error;
+    if (buf && len) {
+        size_t c = std::min(len - 1, s.size());
+        std::memcpy(buf, s.data(), c);
+        buf[c] = 0;
+    }
+    return (int)s.size();
+}
+
+const char* bie_version(void) { return "bie_b200 0.1 sm_100a"; }
+
+int bie_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// ----------------------------- host setup ---------------------------------
+int bie_gausslegendre(int n, double* x, double* w) {
+    return guarded([&] {
+        REQUIRE(n >= 1 && n <= 128 && x && w, "gausslegendre: n must be in [1, 128]");
+        bie::gauss_legendre(n, x, w);
+    });
+}
+
+int bie_best_grid(double W, double H, double alpha, int* m, int* n) {
+    return guarded([&] {
+        REQUIRE(m && n, "best_grid: null output");
+        int rc = bie::best_grid(W, H, alpha, m, n);
+        if (rc == -1) throw Error(BIE_EINVAL, "best_grid: W and H must be positive and alpha >= 1");
+        if (rc != 0) throw Error(BIE_EINVAL, "best_grid: no (m, n) found within search limits");
+    });
+}
+
+int bie_mesh_single_box(double Lx, double Ly, double Lz, int n_quad, double l_ec, double eps_in, double eps_out,
+                        double alpha, bie_mesh** out) {
+    return guarded([&] {
+        REQUIRE(out, "null output");
+        auto h = std::make_unique<bie_mesh>();
+        std::string err;
+        if (bie::mesh_single_box(Lx, Ly, Lz, n_quad, l_ec, eps_in, eps_out, alpha, h->m, err))
+            throw Error(BIE_EINVAL, err);
+        *out = h.release();
+    });
+}
+
+int bie_mesh_multi_box(int n_quad, double l_ec, int nbox, const double* centers, const double* dims,
+                       const double* epses, double eps_out, double alpha, bie_mesh** out) {
+    return guarded([&] {
+        REQUIRE(out && centers && dims && epses, "null argument");
+        auto h = std::make_unique<bie_mesh>();
+        std::string err;
+        if (bie::mesh_multi_box(n_quad, l_ec, nbox, centers, dims, epses, eps_out, alpha, h->m, err))
+            throw Error(BIE_EINVAL, err);
+        *out = h.release();
+    });
+}
+
+int bie_mesh_from_panels(int npanels, int n_quad, const double* corners, const double* normals, const int* is_edge,
+                         const double* eps_in, const double* eps_out, bie_mesh** out) {
+    return guarded([&] {
+        REQUIRE(out && (npanels == 0 || (corners && normals && is_edge && eps_in && eps_out)), "null argument");
+        auto h = std::make_unique<bie_mesh>();
+        std::string err;
+        if (bie::mesh_from_panels(npanels, n_quad, corners, normals, is_edge, eps_in, eps_out, h->m, err))
+            throw Error(BIE_EINVAL, err);
+        *out = h.release();
+    });
+}
+
+int bie_mesh_info(const bie_mesh* m, int64_t* npoints, int* npanels, int* n_quad) {
+    return guarded([&] {
+        REQUIRE(m, "null mesh");
+        if (npoints) *npoints = m->m.npoints();
+        if (npanels) *npanels = m->m.npanels;
+        if (n_quad) *n_quad = m->m.nq;
+    });
+}
+
+int bie_mesh_copy(const bie_mesh* mh, double* corners, double* normals, int* is_edge, double* eps_in, double* eps_out,
+                  double* pts, double* nrm, double* w, double* diag) {
+    return guarded([&] {
+        REQUIRE(mh, "null mesh");
+        const bie::Mesh& m = mh->m;
+        if (corners) std::copy(m.corners.begin(), m.corners.end(), corners);
+        if (normals) std::copy(m.normals.begin(), m.normals.end(), normals);
+        if (is_edge) std::copy(m.is_edge.begin(), m.is_edge.end(), is_edge);
+        if (eps_in) std::copy(m.eps_in.begin(), m.eps_in.end(), eps_in);
+        if (eps_out) std::copy(m.eps_out.begin(), m.eps_out.end(), eps_out);
+        if (pts) std::copy(m.pts.begin(), m.pts.end(), pts);
+        if (w) std::copy(m.w.begin(), m.w.end(), w);
+        const int np = m.nq * m.nq;
+        if (nrm)
+            for (int p = 0; p < m.npanels; ++p)
+                for (int t = 0; t < np; ++t)
+                    for (int c = 0; c < 3; ++c) nrm[3 * ((size_t)p * np + t) + c] = m.normals[3 * p + c];
+        if (diag) m.diag(diag);
+    });
+}
+
+void bie_mesh_destroy(bie_mesh* m) { delete m; }
+
+void bie_near_opts_default(bie_near_opts* o) {
+    if (!o) return;
+    bie::NearOpts d;
+    o->max_order = d.max_order;
+    o->up_tol = d.up_tol;
+    o->correct_edges = d.correct_edges;
+    o->adaptive_atol = d.adaptive_atol;
+    o->adaptive_rtol = d.adaptive_rtol;
+    o->adaptive_n_GL = d.adaptive_n_GL;
+    o->adaptive_max_depth = d.adaptive_max_depth;
+    o->nthreads = d.nthreads;
+}
+
+int bie_near_build(const bie_mesh* m, const bie_near_opts* o, bie_near** out) {
+    return guarded([&] {
+        REQUIRE(m && out, "null argument");
+        bie::NearOpts no;
+        if (o) {
+            no.max_order = o->max_order;
+            no.up_tol = o->up_tol;
+            no.correct_edges = o->correct_edges;
+            no.adaptive_atol = o->adaptive_atol;
+            no.adaptive_rtol = o->adaptive_rtol;
+            no.adaptive_n_GL = o->adaptive_n_GL;
+            no.adaptive_max_depth = o->adaptive_max_depth;
+            no.nthreads = o->nthreads;
+        }
+        auto h = std::make_unique<bie_near>();
+        std::string err;
+        if (bie::near_build(m->m, no, h->n, err)) throw Error(BIE_EINVAL, err);
+        *out = h.release();
+    });
+}
+
+int bie_near_info(const bie_near* n, int64_t* nblocks, int* nb, int* n_ups, int* n_adp, int* hit_max) {
+    return guarded([&] {
+        REQUIRE(n, "null near");
+        if (nblocks) *nblocks = n->n.nblocks();
+        if (nb) *nb = n->n.nb;
+        if (n_ups) *n_ups = (int)n->n.ups_i.size();
+        if (n_adp) *n_adp = (int)n->n.adp_i.size();
+        if (hit_max) *hit_max = n->n.hit_max;
+    });
+}
+
+int bie_near_copy(const bie_near* nh, int32_t* rowptr, int32_t* col, double* val, int32_t* ups_i, int32_t* ups_j,
+                  int32_t* ups_p, int32_t* adp_i, int32_t* adp_j) {
+    return guarded([&] {
+        REQUIRE(nh, "null near");
+        const bie::Near& n = nh->n;
+        if (rowptr) std::copy(n.rowptr.begin(), n.rowptr.end(), rowptr);
+        if (col) std::copy(n.col.begin(), n.col.end(), col);
+        if (val) std::copy(n.val.begin(), n.val.end(), val);
+        if (ups_i) std::copy(n.ups_i.begin(), n.ups_i.end(), ups_i);
+        if (ups_j) std::copy(n.ups_j.begin(), n.ups_j.end(), ups_j);
+        if (ups_p) std::copy(n.ups_p.begin(), n.ups_p.end(), ups_p);
+        if (adp_i) std::copy(n.adp_i.begin(), n.adp_i.end(), adp_i);
+        if (adp_j) std::copy(n.adp_j.begin(), n.adp_j.end(), adp_j);
+    });
+}
+
+void bie_near_destroy(bie_near* n) { delete n; }
+
+// ----------------------------- device geometry -----------------------------
+int bie_geom_create(const double* pts, const double* nrm, const double* w, const double* diag, int64_t n,
+                    int32_t npanels, int32_t nb, const int32_t* rowptr, const int32_t* col, const double* val,
+                    int64_t nblocks, int device, bie_geom** out) {
+    return guarded([&] {
+        REQUIRE(out && pts && nrm && w && diag && n > 0, "geom_create: null array or n <= 0");
+        REQUIRE(nblocks == 0 || (rowptr && col && val && nb > 0 && npanels > 0 && (int64_t)npanels * nb == n),
+                "geom_create: BSR arrays need npanels * nb == n");
+        *out = bie::geom_create(pts, nrm, w, diag, n, npanels, nb, rowptr, col, val, nblocks, device);
+    });
+}
+
+int bie_geom_create_from_mesh(const bie_mesh* mh, const bie_near* nh, int device, bie_geom** out) {
+    return guarded([&] {
+        REQUIRE(mh && out, "null argument");
+        const bie::Mesh& m = mh->m;
+        const int64_t n = m.npoints();
+        REQUIRE(n > 0, "empty mesh");
+        std::vector<double> nrm((size_t)3 * n), diag(n);
+        const int np = m.nq * m.nq;
+        for (int p = 0; p < m.npanels; ++p)
+            for (int t = 0; t < np; ++t)
+                for (int c = 0; c < 3; ++c) nrm[3 * ((size_t)p * np + t) + c] = m.normals[3 * p + c];
+        m.diag(diag.data());
+        const bie::Near* nr = nh ? &nh->n : nullptr;
+        *out = bie::geom_create(m.pts.data(), nrm.data(), m.w.data(), diag.data(), n, m.npanels, np,
+                                nr ? nr->rowptr.data() : nullptr, nr ? nr->col.data() : nullptr,
+                                nr ? nr->val.data() : nullptr, nr ? nr->nblocks() : 0, device);
+    });
+}
+
+int bie_geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes) {
+    return guarded([&] {
+        REQUIRE(g, "null geom");
+        bie::geom_info(g, n, nblocks, bytes);
+    });
+}
+
+void* bie_geom_stream(bie_geom* g) { return g ? bie::geom_stream(g) : nullptr; }
+
+void bie_geom_destroy(bie_geom* g) {
+    if (g) bie::geom_destroy(g);
+}
+
+// ----------------------------- operators ----------------------------------
+int bie_matvec(bie_geom* g, const double* X, double* Y, int32_t k, int32_t precision, uint32_t flags) {
+    return guarded([&] {
+        REQUIRE(g && X && Y && k >= 1, "matvec: bad argument");
+        bie::matvec_host(g, X, Y, k, precision, flags);
+    });
+}
+
+int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int32_t precision, uint32_t flags,
+                      void* stream) {
+    return guarded([&] {
+        REQUIRE(g && dX && dY && k >= 1, "matvec_device: bad argument");
+        bie::matvec_device(g, dX, dY, k, precision, flags, (cudaStream_t)stream);
+    });
+}
+
+int bie_rhs_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* F) {
+    return guarded([&] {
+        REQUIRE(g && src && q && eps_src && F && k >= 1, "rhs_point: bad argument");
+        bie::rhs_point_host(g, src, q, eps_src, k, F);
+    });
+}
+
+int bie_rhs_point_device(bie_geom* g, const double* d_src, const double* d_q, const double* d_eps, int32_t k,
+                         double* dF, void* stream) {
+    return guarded([&] {
+        REQUIRE(g && d_src && d_q && d_eps && dF && k >= 1, "rhs_point_device: bad argument");
+        bie::rhs_point_device(g, d_src, d_q, d_eps, k, dF, (cudaStream_t)stream);
+    });
+}
+
+int bie_potential(bie_geom* g, const double* Sigma, int32_t k, const double* targets, int64_t M, double* phi) {
+    return guarded([&] {
+        REQUIRE(g && Sigma && targets && phi && k >= 1 && M >= 0, "potential: bad argument");
+        bie::potential_host(g, Sigma, k, targets, M, phi);
+    });
+}
+
+int bie_potential_device(bie_geom* g, const double* d_sigma, int32_t k, const double* d_targets, int64_t M,
+                         double* d_phi, void* stream) {
+    return guarded([&] {
+        REQUIRE(g && d_sigma && d_targets && d_phi && k >= 1 && M >= 0, "potential_device: bad argument");
+        bie::potential_device(g, d_sigma, k, d_targets, M, d_phi, (cudaStream_t)stream);
+    });
+}
+
+int bie_energy(bie_geom* g, const double* Sigma, int32_t k, const double* src, const double* q, double* W) {
+    return guarded([&] {
+        REQUIRE(g && Sigma && src && q && W && k >= 1, "energy: bad argument");
+        bie::energy_host(g, Sigma, k, src, q, W);
+    });
+}
+
+// ----------------------------- solvers -------------------------------------
+void bie_solve_opts_default(bie_solve_opts* o) {
+    if (!o) return;
+    o->atol = 0.0;
+    o->rtol = 1e-10;
+    o->itmax = 500;
+    o->restart = 200;
+    o->precision = BIE_FP64;
+    o->inner_rtol = 1e-5;
+    o->max_outer = 8;
+    o->precondition = 0;
+    o->check_every = 1;
+    o->flags = 0;
+}
+
+int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st) {
+    int rc = BIE_OK;
+    int grc = guarded([&] {
+        REQUIRE(g && F && Sigma && k >= 1, "solve: bad argument");
+        bie_solve_opts d;
+        bie_solve_opts_default(&d);
+        rc = bie::solve_host(g, F, Sigma, k, o ? *o : d, st);
+    });
+    return grc != BIE_OK ? grc : rc;
+}
+
+int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o, bie_stats* st,
+                     void* stream) {
+    int rc = BIE_OK;
+    int grc = guarded([&] {
+        REQUIRE(g && dF && dSigma && k >= 1, "solve_device: bad argument");
+        bie_solve_opts d;
+        bie_solve_opts_default(&d);
+        rc = bie::solve_device(g, dF, dSigma, k, o ? *o : d, st, (cudaStream_t)stream);
+    });
+    return grc != BIE_OK ? grc : rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,440 @@
+// CUDA kernels of the layer-potential hot path (sm_100a).
+//
+// Device layout: node coordinates, normals and weights as SoA FP64 arrays of
+// length N; multi-column vectors node-major (X[i * ldx + c], the k values of
+// node i contiguous). Direct sums are split over source chunks; every chunk
+// writes an FP64 partial that the combine kernel reduces in a fixed order
+// (deterministic, no atomics).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bie {
+
+constexpr double kInv4Pi = 0.079577471545947667884;  // 1 / (4 pi)
+constexpr int kTB = 128;  // targets per CTA of the direct-sum kernels (one per thread)
+constexpr int kTS = 128;  // sources per shared-memory tile
+
+struct GeomDev {
+    const double *x, *y, *z;     // node positions
+    const double *nx, *ny, *nz;  // node normals
+    const double* w;             // quadrature weights
+    int64_t n;
+};
+
+// ---------------------------------------------------------------------------
+// K1: FP64 direct D^T sum ("plain").  part[s][i][c0 + c] =
+//   sum_{j in chunk s, j != i} n_i.(x_i - y_j) / |x_i - y_j|^3 * w_j * p_j * X[j][c0 + c]
+// (the 1/(4 pi) is applied by the combine kernel). p = optional right
+// preconditioner (nullptr = 1). Replaces laplace3d_DT (src/kernel/laplace3d.jl:30-40)
+// and the lfmm3d pg=2 far field (src/kernel/laplace3d.jl:100-107).
+// ---------------------------------------------------------------------------
+template <int C>
+__global__ void __launch_bounds__(kTB) k_dt_f64(GeomDev g, const double* __restrict__ X, int ldx, int c0,
+                                                  const double* __restrict__ pre, int64_t chunk,
+                                                  double* __restrict__ part, int ldp) {
+    extern __shared__ double sm[];
+    double* sx = sm;
+    double* sy = sx + kTS;
+    double* sz = sy + kTS;
+    double* sq = sz + kTS;  // [kTS][C]
+    const int64_t i0 = (int64_t)blockIdx.x * kTB;
+    const int64_t i = i0 + threadIdx.x;
+    const bool valid = i < g.n;
+    double xi = 0, yi = 0, zi = 0, n0 = 0, n1 = 0, n2 = 0;
+    if (valid) {
+        xi = g.x[i]; yi = g.y[i]; zi = g.z[i];
+        n0 = g.nx[i]; n1 = g.ny[i]; n2 = g.nz[i];
+    }
+    double acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.0;
+    const int64_t j0 = (int64_t)blockIdx.y * chunk;
+    const int64_t j1 = min(g.n, j0 + chunk);
+    for (int64_t jt = j0; jt < j1; jt += kTS) {
+        const int cnt = (int)min((int64_t)kTS, j1 - jt);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += kTB) {
+            const int64_t j = jt + t;
+            sx[t] = g.x[j]; sy[t] = g.y[j]; sz[t] = g.z[j];
+            double wj = g.w[j] * (pre ? pre[j] : 1.0);
+            const double* xr = X + j * ldx + c0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) sq[t * C + c] = wj * xr[c];
+        }
+        __syncthreads();
+        const bool self_tile = (jt < i0 + kTB) && (jt + cnt > i0);
+        if (!self_tile) {
+#pragma unroll 2
+            for (int t = 0; t < cnt; ++t) {
+                double dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
+                double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                double ri = rsqrt(r2);
+                double nd = fma(n0, dx, fma(n1, dy, n2 * dz));
+                double gk = nd * (ri * ri * ri);
+#pragma unroll
+                for (int c = 0; c < C; ++c) acc[c] = fma(gk, sq[t * C + c], acc[c]);
+            }
+        } else {
+            for (int t = 0; t < cnt; ++t) {
+                if (jt + t == i) continue;
+                double dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
+                double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                double ri = rsqrt(r2);
+                double nd = fma(n0, dx, fma(n1, dy, n2 * dz));
+                double gk = nd * (ri * ri * ri);
+#pragma unroll
+                for (int c = 0; c < C; ++c) acc[c] = fma(gk, sq[t * C + c], acc[c]);
+            }
+        }
+    }
+    if (valid) {
+        double* o = part + ((int64_t)blockIdx.y * g.n + i) * ldp + c0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) o[c] = acc[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2: FP32 direct D^T sum with FP64 tile partials ("refined" inner operator).
+// Coordinates are shifted to the CTA's first target in FP64 before rounding to
+// FP32 (keeps near-pair differences accurate), rsqrt runs on the MUFU pipe,
+// each shared-memory tile accumulates in FP32 and is folded into FP64.
+// ---------------------------------------------------------------------------
+template <int C>
+__global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restrict__ X, int ldx, int c0,
+                                                  const double* __restrict__ pre, int64_t chunk,
+                                                  double* __restrict__ part, int ldp) {
+    extern __shared__ float smf[];
+    float* sx = smf;
+    float* sy = sx + kTS;
+    float* sz = sy + kTS;
+    float* sq = sz + kTS;  // [kTS][C]
+    const int64_t i0 = (int64_t)blockIdx.x * kTB;
+    const int64_t i = i0 + threadIdx.x;
+    const bool valid = i < g.n;
+    const int64_t io = min(i0, g.n - 1);
+    const double ox = g.x[io], oy = g.y[io], oz = g.z[io];
+    float xi = 0.f, yi = 0.f, zi = 0.f, n0 = 0.f, n1 = 0.f, n2 = 0.f;
+    if (valid) {
+        xi = (float)(g.x[i] - ox); yi = (float)(g.y[i] - oy); zi = (float)(g.z[i] - oz);
+        n0 = (float)g.nx[i]; n1 = (float)g.ny[i]; n2 = (float)g.nz[i];
+    }
+    double acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.0;
+    const int64_t j0 = (int64_t)blockIdx.y * chunk;
+    const int64_t j1 = min(g.n, j0 + chunk);
+    for (int64_t jt = j0; jt < j1; jt += kTS) {
+        const int cnt = (int)min((int64_t)kTS, j1 - jt);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += kTB) {
+            const int64_t j = jt + t;
+            sx[t] = (float)(g.x[j] - ox); sy[t] = (float)(g.y[j] - oy); sz[t] = (float)(g.z[j] - oz);
+            double wj = g.w[j] * (pre ? pre[j] : 1.0);
+            const double* xr = X + j * ldx + c0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) sq[t * C + c] = (float)(wj * xr[c]);
+        }
+        __syncthreads();
+        float a32[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) a32[c] = 0.f;
+        const bool self_tile = (jt < i0 + kTB) && (jt + cnt > i0);
+        if (!self_tile) {
+#pragma unroll 4
+            for (int t = 0; t < cnt; ++t) {
+                float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
+                float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                float ri = rsqrtf(r2);
+                float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+                float gk = nd * ri * (ri * ri);
+#pragma unroll
+                for (int c = 0; c < C; ++c) a32[c] = fmaf(gk, sq[t * C + c], a32[c]);
+            }
+        } else {
+            for (int t = 0; t < cnt; ++t) {
+                if (jt + t == i) continue;
+                float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
+                float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                float ri = rsqrtf(r2);
+                float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+                float gk = nd * ri * (ri * ri);
+#pragma unroll
+                for (int c = 0; c < C; ++c) a32[c] = fmaf(gk, sq[t * C + c], a32[c]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] += (double)a32[c];
+    }
+    if (valid) {
+        double* o = part + ((int64_t)blockIdx.y * g.n + i) * ldp + c0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) o[c] = acc[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K6: single-layer potential at targets (FP64):
+//   phi[m][c] = (1/4pi) sum_j w_j S[j][c] / |x_m - y_j|   (laplace3d_pottrg,
+//   src/kernel/laplace3d.jl:69-82). One chunk of sources per blockIdx.y.
+// ---------------------------------------------------------------------------
+template <int C>
+__global__ void __launch_bounds__(kTB) k_pot_f64(GeomDev g, const double* __restrict__ S, int lds, int c0,
+                                                   const double* __restrict__ T /*3 x M*/, int64_t M,
+                                                   int64_t chunk, double* __restrict__ part, int ldp) {
+    extern __shared__ double sm[];
+    double* sx = sm;
+    double* sy = sx + kTS;
+    double* sz = sy + kTS;
+    double* sq = sz + kTS;
+    const int64_t m = (int64_t)blockIdx.x * kTB + threadIdx.x;
+    const bool valid = m < M;
+    double xm = 0, ym = 0, zm = 0;
+    if (valid) { xm = T[3 * m]; ym = T[3 * m + 1]; zm = T[3 * m + 2]; }
+    double acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.0;
+    const int64_t j0 = (int64_t)blockIdx.y * chunk;
+    const int64_t j1 = min(g.n, j0 + chunk);
+    for (int64_t jt = j0; jt < j1; jt += kTS) {
+        const int cnt = (int)min((int64_t)kTS, j1 - jt);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += kTB) {
+            const int64_t j = jt + t;
+            sx[t] = g.x[j]; sy[t] = g.y[j]; sz[t] = g.z[j];
+            const double* sr = S + j * lds + c0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) sq[t * C + c] = g.w[j] * sr[c];
+        }
+        __syncthreads();
+        for (int t = 0; t < cnt; ++t) {
+            double dx = xm - sx[t], dy = ym - sy[t], dz = zm - sz[t];
+            double ri = rsqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[c] = fma(ri, sq[t * C + c], acc[c]);
+        }
+    }
+    if (valid) {
+        double* o = part + ((int64_t)blockIdx.y * M + m) * ldp + c0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) o[c] = acc[c];
+    }
+}
+
+// out[m][c] = scale * sum_s part[s][m][c]
+__global__ void k_reduce_parts(const double* __restrict__ part, int nsplit, int64_t rows, int k, double scale,
+                               double* __restrict__ out) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t tot = rows * k;
+    if (e >= tot) return;
+    double s = 0.0;
+    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
+    out[e] = s * scale;
+}
+
+// ---------------------------------------------------------------------------
+// K4 + K5: combine. Y[i][c] = (1/4pi) sum_s part[s][i][c]       (far field)
+//                          + sum_{blocks (P, Q)} B[r, :] . (p X)[Q rows][c]   (near corrections)
+//                          + t_i p_i X[i][c]                      (diagonal contrast)
+// i = P * nb + r. BSR blocks column-major (val[b*nb*nb + s*nb + r]).
+// Replaces corrections * x (src/kernel/laplace3d_near.jl:417) and the glue loop
+// of mul!(Y, ::BatchedDielectricOperator, X) (src/solver/multi_rhs.jl:120-128).
+// One thread per output; threads of a warp cover consecutive (i, c).
+// ---------------------------------------------------------------------------
+__global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int nsplit,
+                          const double* __restrict__ X, int ldx, const double* __restrict__ pre,
+                          const double* __restrict__ diag, const int32_t* __restrict__ rowptr,
+                          const int32_t* __restrict__ col, const double* __restrict__ val, int nb,
+                          double* __restrict__ Y, int ldy) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    int64_t i = e / k;
+    int c = (int)(e - i * k);
+    double s = 0.0;
+    const int64_t tot = n * (int64_t)k;
+    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
+    s *= kInv4Pi;
+    if (val) {
+        int64_t P = i / nb;
+        int r = (int)(i - P * nb);
+        double a = 0.0;
+        for (int b = rowptr[P]; b < rowptr[P + 1]; ++b) {
+            const double* vb = val + (int64_t)b * nb * nb + r;
+            int64_t base = (int64_t)col[b] * nb;
+            if (pre) {
+                for (int q = 0; q < nb; ++q) a = fma(vb[(int64_t)q * nb], pre[base + q] * X[(base + q) * ldx + c], a);
+            } else {
+                for (int q = 0; q < nb; ++q) a = fma(vb[(int64_t)q * nb], X[(base + q) * ldx + c], a);
+            }
+        }
+        s += a;
+    }
+    if (diag) s += diag[i] * (pre ? pre[i] : 1.0) * X[i * ldx + c];
+    Y[i * ldy + c] = s;
+}
+
+// ---------------------------------------------------------------------------
+// K8: point-source right-hand sides (src/solver/dielectric_box3d.jl:95-104):
+//   F[i][c] = -q_c n_i.(x_i - s_c) / (4 pi |x_i - s_c|^3) / eps_c
+// ---------------------------------------------------------------------------
+__global__ void k_rhs_point(GeomDev g, const double* __restrict__ src /*3 x k*/, const double* __restrict__ q,
+                            const double* __restrict__ eps, int k, double* __restrict__ F) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= g.n * k) return;
+    int64_t i = e / k;
+    int c = (int)(e - i * k);
+    double dx = g.x[i] - src[3 * c], dy = g.y[i] - src[3 * c + 1], dz = g.z[i] - src[3 * c + 2];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double ri = 1.0 / sqrt(r2);
+    double nd = g.nx[i] * dx + g.ny[i] * dy + g.nz[i] * dz;
+    F[e] = -q[c] * (nd * ri * ri * ri * kInv4Pi) / eps[c];
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between Julia's column-major N x k and node-major.
+// ---------------------------------------------------------------------------
+__global__ void k_colmajor_to_nodemajor(const double* __restrict__ A, int64_t n, int k, double* __restrict__ B) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    int64_t i = e / k;
+    int c = (int)(e - i * k);
+    B[e] = A[(int64_t)c * n + i];
+}
+__global__ void k_nodemajor_to_colmajor(const double* __restrict__ B, int64_t n, int k, double* __restrict__ A) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    int c = (int)(e / n);
+    int64_t i = e - (int64_t)c * n;
+    A[e] = B[i * k + c];
+}
+
+// ---------------------------------------------------------------------------
+// K7: device GMRES building blocks (FP64). Multi-column vectors node-major
+// (n x k); each of the k columns runs its own Arnoldi process.
+// ---------------------------------------------------------------------------
+// partial[v][blk][c] = sum_{i in blk rows} A_v[i][c] * B[i][c]  for v < nv
+// (A_v = A + v * strideA). blockDim.x = multiple of k (threads t, t + k, ... share c).
+__global__ void k_dots_partial(const double* __restrict__ A, int64_t strideA, int nv, const double* __restrict__ B,
+                               int64_t n, int k, int64_t rows_per_blk, double* __restrict__ partial, int nblk) {
+    extern __shared__ double red[];
+    const int v = blockIdx.y;
+    const double* Av = A + (int64_t)v * strideA;
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk;
+    const int64_t r1 = min(n, r0 + rows_per_blk);
+    const int64_t e0 = r0 * k, e1 = r1 * k;
+    double s = 0.0;
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) s = fma(Av[e], B[e], s);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    // reduce the groups {c, c + k, c + 2k, ...}; blockDim.x / k is a power of two
+    for (int h = (int)(blockDim.x / k) / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < (unsigned)(h * k)) red[threadIdx.x] += red[threadIdx.x + h * k];
+        __syncthreads();
+    }
+    if (threadIdx.x < (unsigned)k) partial[((int64_t)v * nblk + blockIdx.x) * k + threadIdx.x] = red[threadIdx.x];
+}
+
+// out[v][c] = sum_blk partial[v][blk][c]; mode 0: assign, 1: accumulate, 2: assign sqrt
+__global__ void k_dots_finish(const double* __restrict__ partial, int nv, int nblk, int k, double* __restrict__ out,
+                              int mode) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nv * k) return;
+    int v = e / k, c = e - v * k;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += partial[((int64_t)v * nblk + b) * k + c];
+    out[e] = mode == 1 ? out[e] + s : (mode == 2 ? sqrt(s) : s);
+}
+
+// W[i][c] -= sum_{v < nv} V_v[i][c] h[v][c]
+__global__ void k_gs_update(double* __restrict__ W, const double* __restrict__ V, int64_t strideV, int nv,
+                            const double* __restrict__ h, int64_t n, int k) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    int c = (int)(e % k);
+    double s = W[e];
+    for (int v = 0; v < nv; ++v) s = fma(-V[(int64_t)v * strideV + e], h[v * k + c], s);
+    W[e] = s;
+}
+
+// Y[i][c] = X[i][c] * f[c]; f[c] = 0 where den[c] == 0 (breakdown guard), else num[c] / den[c]
+__global__ void k_scale_cols(const double* __restrict__ X, const double* __restrict__ den, int64_t n, int k,
+                             double* __restrict__ Y) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    int c = (int)(e % k);
+    double d = den[c];
+    Y[e] = d > 0.0 ? X[e] / d : 0.0;
+}
+
+// Y[i][c] = a * X[i][c] + b * Y[i][c] (column mask: only where mask[c] != 0 when mask given)
+__global__ void k_axpby(double a, const double* __restrict__ X, double b, double* __restrict__ Y, int64_t n, int k,
+                        const int* __restrict__ mask) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    if (mask && !mask[e % k]) return;
+    Y[e] = a * X[e] + b * Y[e];
+}
+
+// Givens step of iteration j for every active column (one thread per column).
+// R: [(m+1) x (m+1) x k] column j holds h[0..j+1]; cs/sn: [m x k]; gv: [(m+1) x k].
+__global__ void k_givens(double* __restrict__ R, const double* __restrict__ h /*[(j+1) x k]*/,
+                         const double* __restrict__ hnorm /*[k]*/, double* __restrict__ cs, double* __restrict__ sn,
+                         double* __restrict__ gv, int* __restrict__ active, int* __restrict__ jlast,
+                         const double* __restrict__ eps, double* __restrict__ resid, int j, int m1, int k) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= k) return;
+    if (!active[c]) return;
+    double* Rj = R + ((int64_t)j * m1) * k;  // column j: Rj[i * k + c]
+    for (int i = 0; i <= j; ++i) Rj[i * k + c] = h[i * k + c];
+    Rj[(j + 1) * k + c] = hnorm[c];
+    for (int i = 0; i < j; ++i) {
+        double a = Rj[i * k + c], b = Rj[(i + 1) * k + c];
+        double ci = cs[i * k + c], si = sn[i * k + c];
+        Rj[i * k + c] = ci * a + si * b;
+        Rj[(i + 1) * k + c] = -si * a + ci * b;
+    }
+    double a = Rj[j * k + c], b = Rj[(j + 1) * k + c];
+    double r = hypot(a, b);
+    double cj = r > 0 ? a / r : 1.0, sj = r > 0 ? b / r : 0.0;
+    cs[j * k + c] = cj; sn[j * k + c] = sj;
+    Rj[j * k + c] = r; Rj[(j + 1) * k + c] = 0.0;
+    double gj = gv[j * k + c];
+    gv[(j + 1) * k + c] = -sj * gj;
+    gv[j * k + c] = cj * gj;
+    double res = fabs(gv[(j + 1) * k + c]);
+    resid[c] = res;
+    jlast[c] = j + 1;
+    if (res <= eps[c] || hnorm[c] == 0.0) active[c] = 0;
+}
+
+// y = R^{-1} g for each column over its own jlast[c] (one thread per column).
+__global__ void k_backsolve(const double* __restrict__ R, const double* __restrict__ gv, const int* __restrict__ jlast,
+                            int m1, int k, double* __restrict__ y) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= k) return;
+    int n = jlast[c];
+    for (int i = n - 1; i >= 0; --i) {
+        double s = gv[i * k + c];
+        for (int l = i + 1; l < n; ++l) s -= R[((int64_t)l * m1 + i) * k + c] * y[l * k + c];
+        double d = R[((int64_t)i * m1 + i) * k + c];
+        y[i * k + c] = d != 0.0 ? s / d : 0.0;
+    }
+    for (int i = n; i < m1; ++i) y[i * k + c] = 0.0;
+}
+
+// X[i][c] += p_i * sum_{v < jlast[c]} y[v][c] V_v[i][c]
+__global__ void k_update_solution(double* __restrict__ X, const double* __restrict__ V, int64_t strideV,
+                                  const double* __restrict__ y, const int* __restrict__ jlast, int jmax,
+                                  const double* __restrict__ pre, int64_t n, int k) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    int c = (int)(e % k);
+    int nv = min(jlast[c], jmax);
+    double s = 0.0;
+    for (int v = 0; v < nv; ++v) s = fma(y[v * k + c], V[(int64_t)v * strideV + e], s);
+    if (pre) s *= pre[e / k];
+    X[e] += s;
+}
+
+}  // namespace bie

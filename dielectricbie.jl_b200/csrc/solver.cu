@@ -1,0 +1,649 @@
+// Device-resident geometry, layer-potential operators and the device GMRES /
+// iterative-refinement solvers of libbie_b200.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "kernels.cuh"
+#include "solver.h"
+
+struct bie_geom {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sms = 148;
+    int64_t n = 0;
+    int32_t npanels = 0, nb = 0;
+    int64_t nblocks = 0;
+    size_t geom_bytes = 0;
+    bie::Buf x, y, z, nx, ny, nz, w, diag, pinv;
+    bie::Buf rowptr, col, val;
+    // operator workspace
+    bie::Buf part, small;
+    // solver workspace
+    bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace bie {
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) BIE_CK(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+inline unsigned grid1(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+GeomDev gdev(const bie_geom* g) {
+    return GeomDev{g->x.as<double>(), g->y.as<double>(), g->z.as<double>(), g->nx.as<double>(),
+                   g->ny.as<double>(), g->nz.as<double>(), g->w.as<double>(), g->n};
+}
+
+template <class T>
+void upload(bie::Buf& b, const T* src, size_t count, cudaStream_t s) {
+    b.ensure(sizeof(T) * std::max<size_t>(count, 1));
+    if (count) BIE_CK(cudaMemcpyAsync(b.p, src, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+}
+
+// --------------------------- direct-sum launchers --------------------------
+enum class Kern { DT64, DT32, POT64 };
+
+template <int C>
+void* kern_ptr(Kern kind) {
+    switch (kind) {
+        case Kern::DT64: return (void*)k_dt_f64<C>;
+        case Kern::DT32: return (void*)k_dt_f32<C>;
+        default: return (void*)k_pot_f64<C>;
+    }
+}
+
+template <int C>
+size_t kern_smem(Kern kind) {
+    return (size_t)(3 + C) * kTS * (kind == Kern::DT32 ? sizeof(float) : sizeof(double));
+}
+
+// occupancy (CTAs per SM) of one instantiation; also raises the dynamic smem limit once
+template <int C>
+int kern_occ(Kern kind) {
+    static int cache[3] = {0, 0, 0};
+    int idx = (int)kind;
+    if (cache[idx]) return cache[idx];
+    size_t sm = kern_smem<C>(kind);
+    void* f = kern_ptr<C>(kind);
+    if (sm > 48 * 1024) BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int occ = 0;
+    BIE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kTB, sm));
+    cache[idx] = std::max(occ, 1);
+    return cache[idx];
+}
+
+struct Split {
+    int nsplit;
+    int64_t chunk;
+};
+
+Split choose_split(int64_t rows, int64_t nsrc, int sms, int occ) {
+    int64_t nblkx = (rows + kTB - 1) / kTB;
+    int64_t want = (int64_t)sms * occ * 4;
+    int64_t maxs = std::max<int64_t>(1, (nsrc + kTS - 1) / kTS);
+    int64_t ns = std::min(maxs, std::max<int64_t>(1, (want + nblkx - 1) / nblkx));
+    int64_t chunk = (nsrc + ns - 1) / ns;
+    chunk = (chunk + kTS - 1) / kTS * kTS;
+    ns = std::max<int64_t>(1, (nsrc + chunk - 1) / chunk);
+    return Split{(int)ns, chunk};
+}
+
+template <int C>
+void launch_direct(Kern kind, const GeomDev& g, const double* X, int ldx, int c0, const double* pre,
+                   const double* T, int64_t M, Split sp, double* part, int ldp, cudaStream_t s) {
+    size_t sm = kern_smem<C>(kind);
+    kern_occ<C>(kind);  // sets the smem attribute
+    int64_t rows = kind == Kern::POT64 ? M : g.n;
+    dim3 grid((unsigned)((rows + kTB - 1) / kTB), (unsigned)sp.nsplit);
+    if (kind == Kern::DT64)
+        k_dt_f64<C><<<grid, kTB, sm, s>>>(g, X, ldx, c0, pre, sp.chunk, part, ldp);
+    else if (kind == Kern::DT32)
+        k_dt_f32<C><<<grid, kTB, sm, s>>>(g, X, ldx, c0, pre, sp.chunk, part, ldp);
+    else
+        k_pot_f64<C><<<grid, kTB, sm, s>>>(g, X, ldx, c0, T, M, sp.chunk, part, ldp);
+    BIE_CK(cudaGetLastError());
+}
+
+int occ_for(Kern kind, int C) {
+    switch (C) {
+        case 64: return kern_occ<64>(kind);
+        case 32: return kern_occ<32>(kind);
+        case 16: return kern_occ<16>(kind);
+        case 8: return kern_occ<8>(kind);
+        case 4: return kern_occ<4>(kind);
+        case 2: return kern_occ<2>(kind);
+        default: return kern_occ<1>(kind);
+    }
+}
+
+int pick_C(int rem) {
+    static const int cs[] = {64, 32, 16, 8, 4, 2, 1};
+    for (int c : cs)
+        if (c <= rem) return c;
+    return 1;
+}
+
+// Runs the direct sum for all k columns into g->part; returns the split used.
+Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const double* pre, const double* T,
+                 int64_t M, cudaStream_t s) {
+    GeomDev gd = gdev(g);
+    int64_t rows = kind == Kern::POT64 ? M : g->n;
+    int Cmax = pick_C(k);
+    Split sp = choose_split(rows, g->n, g->sms, occ_for(kind, Cmax));
+    g->part.ensure(sizeof(double) * (size_t)sp.nsplit * std::max<int64_t>(rows, 1) * k);
+    double* part = g->part.as<double>();
+    for (int c0 = 0; c0 < k;) {
+        int C = pick_C(k - c0);
+        switch (C) {
+            case 64: launch_direct<64>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+            case 32: launch_direct<32>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+            case 16: launch_direct<16>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+            case 8: launch_direct<8>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+            case 4: launch_direct<4>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+            case 2: launch_direct<2>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+            default: launch_direct<1>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
+        }
+        c0 += C;
+    }
+    return sp;
+}
+
+// Y = A(prec) (p .* X), node-major n x k (ldx = ldy = k).
+void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
+              cudaStream_t s) {
+    Kern kind;
+    if (prec == BIE_FP64) kind = Kern::DT64;
+    else if (prec == BIE_FP32) kind = Kern::DT32;
+    else throw Error(BIE_EUNSUPPORTED, "precision BIE_BF16X3 is not available in this build");
+    Split sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
+    const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
+    const bool dg = !(flags & BIE_NO_DIAG);
+    k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
+                                              dg ? g->diag.as<double>() : nullptr,
+                                              corr ? g->rowptr.as<int32_t>() : nullptr,
+                                              corr ? g->col.as<int32_t>() : nullptr,
+                                              corr ? g->val.as<double>() : nullptr, g->nb, Y, k);
+    BIE_CK(cudaGetLastError());
+}
+
+// ------------------------------ reductions ---------------------------------
+struct DotPlan {
+    int bs, nblk;
+    int64_t rows_per_blk;
+};
+
+DotPlan dot_plan(int64_t n, int k, int nv) {
+    int groups = 1;
+    while (k * groups * 2 <= 256) groups *= 2;
+    DotPlan p;
+    p.bs = k * groups;
+    if (p.bs < 32 && k <= 256) p.bs = k * groups;  // k > 256 handled by the caller (unsupported)
+    int64_t elems = n * (int64_t)k;
+    int64_t nblk = std::max<int64_t>(1, std::min<int64_t>(1024 / std::max(1, nv) + 1, (elems + p.bs * 16 - 1) / (p.bs * 16)));
+    nblk = std::min<int64_t>(nblk, n);
+    p.rows_per_blk = (n + nblk - 1) / nblk;
+    p.nblk = (int)((n + p.rows_per_blk - 1) / p.rows_per_blk);
+    return p;
+}
+
+// out[v][c] = sum_i A_v[i][c] B[i][c] for v < nv (mode: 0 assign, 1 accumulate, 2 sqrt)
+void dots(bie_geom* g, const double* A, int64_t strideA, int nv, const double* B, int k, double* out, int mode,
+          cudaStream_t s) {
+    DotPlan p = dot_plan(g->n, k, nv);
+    g->dpart.ensure(sizeof(double) * (size_t)p.nblk * nv * k);
+    dim3 grid(p.nblk, nv);
+    k_dots_partial<<<grid, p.bs, p.bs * sizeof(double), s>>>(A, strideA, nv, B, g->n, k, p.rows_per_blk,
+                                                            g->dpart.as<double>(), p.nblk);
+    BIE_CK(cudaGetLastError());
+    k_dots_finish<<<grid1(nv * k), 256, 0, s>>>(g->dpart.as<double>(), nv, p.nblk, k, out, mode);
+    BIE_CK(cudaGetLastError());
+}
+
+void col_norms(bie_geom* g, const double* X, int k, double* out, cudaStream_t s) {
+    dots(g, X, 0, 1, X, k, out, 2, s);
+}
+
+template <class T>
+void d2h(T* dst, const void* src, size_t count, cudaStream_t s) {
+    BIE_CK(cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+}
+
+// ------------------------------- GMRES -------------------------------------
+struct GmresResult {
+    int iters = 0;       // iterations (= operator applications inside the Arnoldi loop)
+    int matvecs = 0;     // all operator applications incl. restart residuals
+    bool all_converged = false;
+    std::vector<int> col_iters;
+};
+
+// Solves A(prec) (p .* u) = r, x = p .* u for the columns flagged in `active0`;
+// dx (node-major n x k) receives the solution (zeroed first). eps[c] is the
+// absolute residual tolerance of column c. Each column runs its own Arnoldi
+// process with classical Gram-Schmidt applied twice; converged columns are frozen.
+GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
+                  const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, int check_every,
+                  cudaStream_t s) {
+    const int64_t n = g->n;
+    const int64_t nk = n * (int64_t)k;
+    m = std::max(1, std::min(m, itmax));
+    const int m1 = m + 1;
+    g->V.ensure(sizeof(double) * (size_t)m1 * nk);
+    g->W.ensure(sizeof(double) * nk);
+    g->rr.ensure(sizeof(double) * nk);
+    g->R.ensure(sizeof(double) * (size_t)m1 * m1 * k);
+    g->gv.ensure(sizeof(double) * (size_t)m1 * k);
+    g->cs.ensure(sizeof(double) * (size_t)m1 * k);
+    g->sn.ensure(sizeof(double) * (size_t)m1 * k);
+    g->h.ensure(sizeof(double) * (size_t)m1 * k);
+    g->h2.ensure(sizeof(double) * (size_t)m1 * k);
+    g->hn.ensure(sizeof(double) * k);
+    g->beta.ensure(sizeof(double) * k);
+    g->eps.ensure(sizeof(double) * k);
+    g->active.ensure(sizeof(int) * k);
+    g->jlast.ensure(sizeof(int) * k);
+    g->yv.ensure(sizeof(double) * (size_t)m1 * k);
+    g->resid.ensure(sizeof(double) * k);
+    double* V = g->V.as<double>();
+    double* W = g->W.as<double>();
+    BIE_CK(cudaMemsetAsync(dx, 0, sizeof(double) * nk, s));
+    upload(g->eps, eps.data(), k, s);
+    GmresResult res;
+    res.col_iters.assign(k, 0);
+    std::vector<double> hb(k), g0((size_t)k);
+    std::vector<int> act(k), jl(k);
+    bool first = true;
+    int it = 0;
+    while (true) {
+        // residual of the current cycle
+        const double* r = dr;
+        if (!first) {
+            apply_op(g, dx, W, k, prec, flags, pre, s);
+            ++res.matvecs;
+            BIE_CK(cudaMemcpyAsync(g->rr.p, dr, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
+            k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, W, 1.0, g->rr.as<double>(), n, k, nullptr);
+            r = g->rr.as<double>();
+        }
+        col_norms(g, r, k, g->beta.as<double>(), s);
+        d2h(hb.data(), g->beta.p, k, s);
+        int nact = 0;
+        for (int c = 0; c < k; ++c) {
+            act[c] = active0[c] && hb[c] > eps[c] ? 1 : 0;
+            nact += act[c];
+        }
+        if (nact == 0) {
+            res.all_converged = true;
+            break;
+        }
+        if (it >= itmax) break;
+        upload(g->active, act.data(), k, s);
+        BIE_CK(cudaMemsetAsync(g->jlast.p, 0, sizeof(int) * k, s));
+        BIE_CK(cudaMemsetAsync(g->gv.p, 0, sizeof(double) * m1 * k, s));
+        BIE_CK(cudaMemcpyAsync(g->gv.p, g->beta.p, sizeof(double) * k, cudaMemcpyDeviceToDevice, s));
+        k_scale_cols<<<grid1(nk), 256, 0, s>>>(r, g->beta.as<double>(), n, k, V);
+        int j = 0;
+        bool any = true;
+        for (; j < m && it < itmax; ++j) {
+            double* Vj = V + (size_t)j * nk;
+            apply_op(g, Vj, W, k, prec, flags, pre, s);
+            ++res.matvecs;
+            // classical Gram-Schmidt, twice
+            dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
+            k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+            dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
+            k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h2.as<double>(), n, k);
+            k_axpby<<<grid1((j + 1) * k), 256, 0, s>>>(1.0, g->h2.as<double>(), 1.0, g->h.as<double>(), j + 1, k,
+                                                        nullptr);
+            col_norms(g, W, k, g->hn.as<double>(), s);
+            k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
+            k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->hn.as<double>(),
+                                                 g->cs.as<double>(), g->sn.as<double>(), g->gv.as<double>(),
+                                                 g->active.as<int>(), g->jlast.as<int>(), g->eps.as<double>(),
+                                                 g->resid.as<double>(), j, m1, k);
+            BIE_CK(cudaGetLastError());
+            ++it;
+            if ((j + 1) % std::max(1, check_every) == 0 || j + 1 == m || it >= itmax) {
+                d2h(act.data(), g->active.p, k, s);
+                any = false;
+                for (int c = 0; c < k; ++c) any = any || act[c];
+                if (!any) {
+                    ++j;
+                    break;
+                }
+            }
+        }
+        k_backsolve<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->gv.as<double>(), g->jlast.as<int>(), m1, k,
+                                                 g->yv.as<double>());
+        k_update_solution<<<grid1(nk), 256, 0, s>>>(dx, V, nk, g->yv.as<double>(), g->jlast.as<int>(), m, pre, n, k);
+        BIE_CK(cudaGetLastError());
+        d2h(jl.data(), g->jlast.p, k, s);
+        for (int c = 0; c < k; ++c) res.col_iters[c] += jl[c];
+        d2h(act.data(), g->active.p, k, s);
+        any = false;
+        for (int c = 0; c < k; ++c) any = any || act[c];
+        if (!any) {
+            res.all_converged = true;
+            break;
+        }
+        if (it >= itmax) break;
+        first = false;  // restart from the true residual of the current iterate
+    }
+    res.iters = it;
+    return res;
+}
+
+void check_prec(int prec) {
+    if (prec != BIE_FP64 && prec != BIE_FP32 && prec != BIE_BF16X3) throw Error(BIE_EINVAL, "unknown precision");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// geometry lifetime
+// ---------------------------------------------------------------------------
+bie_geom* geom_create(const double* pts, const double* nrm, const double* w, const double* diag, int64_t n,
+                      int32_t npanels, int32_t nb, const int32_t* rowptr, const int32_t* col, const double* val,
+                      int64_t nblocks, int device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        throw Error(BIE_ENODEVICE, "no CUDA device available (libbie_b200 has no CPU fallback)");
+    }
+    if (device < 0 || device >= ndev) throw Error(BIE_EINVAL, "device ordinal out of range");
+    DeviceGuard dg(device);
+    std::unique_ptr<bie_geom> g(new bie_geom());
+    g->device = device;
+    BIE_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    BIE_CK(cudaEventCreate(&g->ev0));
+    BIE_CK(cudaEventCreate(&g->ev1));
+    BIE_CK(cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, device));
+    g->n = n;
+    g->npanels = npanels;
+    g->nb = nb;
+    g->nblocks = nblocks;
+    std::vector<double> col3((size_t)n);
+    cudaStream_t s = g->stream;
+    bie::Buf* xs[3] = {&g->x, &g->y, &g->z};
+    bie::Buf* ns[3] = {&g->nx, &g->ny, &g->nz};
+    for (int c = 0; c < 3; ++c) {
+        for (int64_t i = 0; i < n; ++i) col3[i] = pts[3 * i + c];
+        upload(*xs[c], col3.data(), n, s);
+        BIE_CK(cudaStreamSynchronize(s));
+        for (int64_t i = 0; i < n; ++i) col3[i] = nrm[3 * i + c];
+        upload(*ns[c], col3.data(), n, s);
+        BIE_CK(cudaStreamSynchronize(s));
+    }
+    upload(g->w, w, n, s);
+    upload(g->diag, diag, n, s);
+    for (int64_t i = 0; i < n; ++i) col3[i] = diag[i] != 0.0 ? 1.0 / diag[i] : 1.0;
+    upload(g->pinv, col3.data(), n, s);
+    if (nblocks > 0) {
+        upload(g->rowptr, rowptr, (size_t)npanels + 1, s);
+        upload(g->col, col, nblocks, s);
+        upload(g->val, val, (size_t)nblocks * nb * nb, s);
+    }
+    BIE_CK(cudaStreamSynchronize(s));
+    g->geom_bytes = sizeof(double) * (size_t)n * 9 + (nblocks > 0 ? (sizeof(int32_t) * ((size_t)npanels + 1 + nblocks) +
+                                                                     sizeof(double) * (size_t)nblocks * nb * nb)
+                                                                  : 0);
+    return g.release();
+}
+
+void geom_destroy(bie_geom* g) {
+    {
+        DeviceGuard dg(g->device);
+        if (g->stream) cudaStreamSynchronize(g->stream);
+        bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->rowptr,
+                           &g->col, &g->val, &g->part, &g->small, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
+                           &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
+                           &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
+        for (auto* b : all) b->release();
+        if (g->ev0) cudaEventDestroy(g->ev0);
+        if (g->ev1) cudaEventDestroy(g->ev1);
+        if (g->stream) cudaStreamDestroy(g->stream);
+    }
+    delete g;
+}
+
+void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes) {
+    if (n) *n = g->n;
+    if (nblocks) *nblocks = g->nblocks;
+    if (bytes) *bytes = g->geom_bytes;
+}
+
+void* geom_stream(bie_geom* g) { return (void*)g->stream; }
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+void matvec_device(bie_geom* g, const double* dX, double* dY, int k, int precision, uint32_t flags, cudaStream_t s) {
+    check_prec(precision);
+    DeviceGuard dg(g->device);
+    if (!s) s = g->stream;
+    apply_op(g, dX, dY, k, precision, flags, nullptr, s);
+}
+
+void matvec_host(bie_geom* g, const double* X, double* Y, int k, int precision, uint32_t flags) {
+    check_prec(precision);
+    DeviceGuard dg(g->device);
+    cudaStream_t s = g->stream;
+    const int64_t nk = g->n * (int64_t)k;
+    g->io_a.ensure(sizeof(double) * nk);
+    g->io_b.ensure(sizeof(double) * nk);
+    g->xo.ensure(sizeof(double) * nk);
+    BIE_CK(cudaMemcpyAsync(g->io_a.p, X, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+    k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    apply_op(g, g->io_b.as<double>(), g->xo.as<double>(), k, precision, flags, nullptr, s);
+    k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->xo.as<double>(), g->n, k, g->io_a.as<double>());
+    BIE_CK(cudaGetLastError());
+    BIE_CK(cudaMemcpyAsync(Y, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+}
+
+void rhs_point_device(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* F,
+                      cudaStream_t s) {
+    DeviceGuard dg(g->device);
+    if (!s) s = g->stream;
+    k_rhs_point<<<grid1(g->n * k), 256, 0, s>>>(gdev(g), src, q, eps, k, F);
+    BIE_CK(cudaGetLastError());
+}
+
+void rhs_point_host(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* F) {
+    DeviceGuard dg(g->device);
+    cudaStream_t s = g->stream;
+    std::vector<double> packed((size_t)5 * k);
+    std::copy(src, src + 3 * k, packed.begin());
+    std::copy(q, q + k, packed.begin() + 3 * k);
+    std::copy(eps, eps + k, packed.begin() + 4 * k);
+    upload(g->small, packed.data(), packed.size(), s);
+    const int64_t nk = g->n * (int64_t)k;
+    g->io_a.ensure(sizeof(double) * nk);
+    g->io_b.ensure(sizeof(double) * nk);
+    const double* d = g->small.as<double>();
+    k_rhs_point<<<grid1(nk), 256, 0, s>>>(gdev(g), d, d + 3 * k, d + 4 * k, k, g->io_b.as<double>());
+    k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->io_b.as<double>(), g->n, k, g->io_a.as<double>());
+    BIE_CK(cudaGetLastError());
+    BIE_CK(cudaMemcpyAsync(F, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+}
+
+void potential_device(bie_geom* g, const double* S, int k, const double* T, int64_t M, double* phi, cudaStream_t s) {
+    DeviceGuard dg(g->device);
+    if (!s) s = g->stream;
+    if (M == 0) return;
+    Split sp = direct_sum(g, Kern::POT64, S, k, k, nullptr, T, M, s);
+    k_reduce_parts<<<grid1(M * k), 256, 0, s>>>(g->part.as<double>(), sp.nsplit, M, k, kInv4Pi, phi);
+    BIE_CK(cudaGetLastError());
+}
+
+void potential_host(bie_geom* g, const double* S, int k, const double* T, int64_t M, double* phi) {
+    DeviceGuard dg(g->device);
+    cudaStream_t s = g->stream;
+    if (M == 0) return;
+    const int64_t nk = g->n * (int64_t)k;
+    g->io_a.ensure(sizeof(double) * std::max<int64_t>(nk, M * k));
+    g->io_b.ensure(sizeof(double) * nk);
+    g->xo.ensure(sizeof(double) * M * k);
+    upload(g->small, T, (size_t)3 * M, s);
+    BIE_CK(cudaMemcpyAsync(g->io_a.p, S, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+    k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    potential_device(g, g->io_b.as<double>(), k, g->small.as<double>(), M, g->xo.as<double>(), s);
+    k_nodemajor_to_colmajor<<<grid1(M * k), 256, 0, s>>>(g->xo.as<double>(), M, k, g->io_a.as<double>());
+    BIE_CK(cudaGetLastError());
+    BIE_CK(cudaMemcpyAsync(phi, g->io_a.p, sizeof(double) * M * k, cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+}
+
+void energy_host(bie_geom* g, const double* S, int k, const double* src, const double* q, double* W) {
+    std::vector<double> phi((size_t)k * k);
+    potential_host(g, S, k, src, k, phi.data());
+    for (int c = 0; c < k; ++c) W[c] = 0.5 * q[c] * phi[(size_t)c * k + c];  // column c at target c
+}
+
+// ---------------------------------------------------------------------------
+// solvers
+// ---------------------------------------------------------------------------
+int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_solve_opts& o, bie_stats* st,
+                 cudaStream_t s) {
+    check_prec(o.precision);
+    if (o.itmax < 1 || o.restart < 1 || !(o.rtol >= 0) || !(o.atol >= 0)) throw Error(BIE_EINVAL, "bad solver options");
+    if (k > 256) throw Error(BIE_EUNSUPPORTED, "at most 256 right-hand sides per solve");
+    DeviceGuard dg(g->device);
+    if (!s) s = g->stream;
+    const int64_t n = g->n, nk = n * (int64_t)k;
+    const double* pre = o.precondition ? g->pinv.as<double>() : nullptr;
+    BIE_CK(cudaEventRecord(g->ev0, s));
+    // ||F_c|| and the per-column tolerance atol + rtol ||F_c|| (Krylov.jl stopping rule)
+    g->small.ensure(sizeof(double) * (size_t)std::max(2 * k, 8));
+    col_norms(g, dF, k, g->small.as<double>(), s);
+    std::vector<double> fn(k), tol(k);
+    d2h(fn.data(), g->small.p, k, s);
+    for (int c = 0; c < k; ++c) tol[c] = o.atol + o.rtol * fn[c];
+    std::vector<char> act(k, 1);
+    int iters = 0, outer = 0, f64mv = 0, lpmv = 0;
+    bool converged = false;
+    std::vector<int> col_it(k, 0);
+    std::vector<double> rel(k, 0.0);
+    bool have_true_resid = false;
+    g->rr.ensure(sizeof(double) * nk);
+    g->dd.ensure(sizeof(double) * nk);
+    g->xo.ensure(sizeof(double) * nk);
+    double* rbuf = g->xo.as<double>();  // outer residual F - A x
+    if (o.precision == BIE_FP64) {
+        GmresResult r = gmres(g, dF, dX, k, BIE_FP64, o.flags, pre, tol, act, o.itmax, o.restart, o.check_every, s);
+        iters = r.iters;
+        outer = 1;
+        f64mv = r.matvecs;
+        converged = r.all_converged;
+        col_it = r.col_iters;
+    } else {
+        BIE_CK(cudaMemsetAsync(dX, 0, sizeof(double) * nk, s));
+        std::vector<double> rn = fn, eps_in(k);
+        const double* rhs = dF;
+        for (int it_out = 0;; ++it_out) {
+            if (it_out > 0) {
+                // FP64 outer residual r = F - A x
+                apply_op(g, dX, rbuf, k, BIE_FP64, o.flags, nullptr, s);
+                ++f64mv;
+                k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, dF, -1.0, rbuf, n, k, nullptr);
+                col_norms(g, rbuf, k, g->small.as<double>(), s);
+                d2h(rn.data(), g->small.p, k, s);
+                rhs = rbuf;
+                have_true_resid = true;
+            }
+            int nact = 0;
+            for (int c = 0; c < k; ++c) {
+                act[c] = rn[c] > tol[c] ? 1 : 0;
+                nact += act[c];
+                rel[c] = fn[c] > 0 ? rn[c] / fn[c] : 0.0;
+            }
+            if (nact == 0) {
+                converged = true;
+                break;
+            }
+            if (it_out >= o.max_outer || iters >= o.itmax) break;
+            for (int c = 0; c < k; ++c) eps_in[c] = std::max(o.inner_rtol * rn[c], 0.5 * tol[c]);
+            GmresResult r = gmres(g, rhs, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
+                                  o.itmax - iters, o.restart, o.check_every, s);
+            iters += r.iters;
+            lpmv += r.matvecs;
+            for (int c = 0; c < k; ++c) col_it[c] += r.col_iters[c];
+            upload(g->active, std::vector<int>(act.begin(), act.end()).data(), k, s);
+            k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, g->dd.as<double>(), 1.0, dX, n, k, g->active.as<int>());
+            BIE_CK(cudaGetLastError());
+            ++outer;
+        }
+    }
+    const bool verify = !(o.flags & 4u) && (st != nullptr);
+    if (verify && !have_true_resid) {
+        apply_op(g, dX, rbuf, k, BIE_FP64, o.flags, nullptr, s);
+        ++f64mv;
+        k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, dF, -1.0, rbuf, n, k, nullptr);
+        std::vector<double> rn(k);
+        col_norms(g, rbuf, k, g->small.as<double>(), s);
+        d2h(rn.data(), g->small.p, k, s);
+        bool all = true;
+        for (int c = 0; c < k; ++c) {
+            rel[c] = fn[c] > 0 ? rn[c] / fn[c] : 0.0;
+            all = all && rn[c] <= tol[c] * (1.0 + 1e-6) + 1e-300;
+        }
+        if (o.precision == BIE_FP64) converged = converged && all;
+    }
+    BIE_CK(cudaEventRecord(g->ev1, s));
+    BIE_CK(cudaEventSynchronize(g->ev1));
+    float ms = 0.f;
+    BIE_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    if (st) {
+        st->iterations = iters;
+        st->outer = outer;
+        st->fp64_matvecs = f64mv;
+        st->lowp_matvecs = lpmv;
+        st->converged = converged ? 1 : 0;
+        double mx = 0.0;
+        for (int c = 0; c < k; ++c) mx = std::max(mx, rel[c]);
+        st->max_rel_resid = mx;
+        st->seconds = ms * 1e-3;
+        if (st->col_iterations)
+            for (int c = 0; c < k; ++c) st->col_iterations[c] = col_it[c];
+        if (st->col_resid)
+            for (int c = 0; c < k; ++c) st->col_resid[c] = rel[c];
+    }
+    return converged ? BIE_OK : BIE_ENOCONV;
+}
+
+int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_solve_opts& o, bie_stats* st) {
+    DeviceGuard dg(g->device);
+    cudaStream_t s = g->stream;
+    const int64_t nk = g->n * (int64_t)k;
+    g->io_a.ensure(sizeof(double) * nk);
+    g->io_b.ensure(sizeof(double) * nk);
+    g->sol.ensure(sizeof(double) * nk);  // output buffer, never aliased by the solver's scratch
+    BIE_CK(cudaMemcpyAsync(g->io_a.p, F, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
+    k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    int rc = solve_device(g, g->io_b.as<double>(), g->sol.as<double>(), k, o, st, s);
+    k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->sol.as<double>(), g->n, k, g->io_a.as<double>());
+    BIE_CK(cudaGetLastError());
+    BIE_CK(cudaMemcpyAsync(Sigma, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+    return rc;
+}
+
+}  // namespace bie

@@ -1,0 +1,50 @@
+// Internal declarations shared by the ABI layer and the device orchestration.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/bie_b200.h"
+
+namespace bie {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define BIE_CK(call) ::bie::cuda_check((call), #call)
+
+// Grow-only device buffer owned by a geometry handle.
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t need);
+    void release();
+    template <class T>
+    T* as() const { return (T*)p; }
+};
+
+bie_geom* geom_create(const double* pts, const double* nrm, const double* w, const double* diag, int64_t n,
+                      int32_t npanels, int32_t nb, const int32_t* rowptr, const int32_t* col, const double* val,
+                      int64_t nblocks, int device);
+void geom_destroy(bie_geom* g);
+void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes);
+void* geom_stream(bie_geom* g);
+
+void matvec_host(bie_geom* g, const double* X, double* Y, int k, int precision, uint32_t flags);
+void matvec_device(bie_geom* g, const double* dX, double* dY, int k, int precision, uint32_t flags, cudaStream_t s);
+void rhs_point_host(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* F);
+void rhs_point_device(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* F,
+                      cudaStream_t s);
+void potential_host(bie_geom* g, const double* S, int k, const double* T, int64_t M, double* phi);
+void potential_device(bie_geom* g, const double* S, int k, const double* T, int64_t M, double* phi, cudaStream_t s);
+void energy_host(bie_geom* g, const double* S, int k, const double* src, const double* q, double* W);
+int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_solve_opts& o, bie_stats* st);
+int solve_device(bie_geom* g, const double* dF, double* dSigma, int k, const bie_solve_opts& o, bie_stats* st,
+                 cudaStream_t s);
+
+}  // namespace bie

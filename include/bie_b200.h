@@ -1,0 +1,209 @@
+/*
+ * bie_b200.h -- C ABI of libbie_b200.so, the B200 (sm_100a) layer-potential
+ * library for the dielectric boundary-integral equation of DielectricBIE.jl.
+ *
+ * Conventions
+ *   - Host arrays are borrowed for the duration of a call, Float64, in Julia's
+ *     column-major layout: points/normals 3 x N (x, y, z of node i contiguous),
+ *     multi-column vectors N x k (column c contiguous).
+ *   - Device arrays passed to the *_device entry points use the library's
+ *     device layout: N x k row-major ("node-major", the k values of node i
+ *     contiguous). For k = 1 the two layouts coincide.
+ *   - Every entry point returns a bie_status; no exception crosses the ABI. The
+ *     message of the last failure on the calling thread is kept for
+ *     bie_last_error.
+ *   - A bie_geom is bound to one CUDA device and one stream; calls on distinct
+ *     handles may run concurrently from different threads, calls on one handle
+ *     must be serialised by the caller.
+ *   - Node order is the reference's: panels in mesher order, within a panel the
+ *     (b - a) Gauss index outer and the (d - a) index inner
+ *     (src/shape/box3d.jl:44-52, src/core/panels.jl:87-115).
+ */
+#ifndef BIE_B200_H
+#define BIE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    BIE_OK = 0,
+    BIE_EINVAL = 1,        /* bad argument (sizes, null pointers, options) */
+    BIE_ENOMEM = 2,        /* device or host allocation failed */
+    BIE_ECUDA = 3,         /* CUDA runtime error (message in bie_last_error) */
+    BIE_ENOCONV = 4,       /* solver stopped at itmax before reaching the tolerance */
+    BIE_ETIMEOUT = 5,      /* a bounded device wait ran out (kernel returned early) */
+    BIE_EUNSUPPORTED = 6,  /* valid request outside what this build supports */
+    BIE_ENODEVICE = 7      /* no CUDA device (the library has no CPU fallback) */
+} bie_status;
+
+/* Arithmetic of the layer-potential sum inside a matvec / solve. */
+typedef enum {
+    BIE_FP64 = 0,   /* plain: FP64 end to end */
+    BIE_FP32 = 1,   /* FP32 direct sum (FP64 tile partials), FP64 corrections/diag */
+    BIE_BF16X3 = 2  /* split-BF16 three-term tensor-core RHS contraction (k >= 16),
+                       FP32 kernel tiles, FP64 corrections/diag */
+} bie_precision;
+
+/* matvec flags */
+#define BIE_NO_CORRECTIONS 1u /* skip the near-field correction blocks */
+#define BIE_NO_DIAG 2u        /* skip the diagonal contrast term */
+
+/* Copies the message of the last failed call on this thread (always NUL-terminated).
+ * Returns the full message length. */
+int bie_last_error(char* buf, size_t len);
+/* Library version string, e.g. "bie_b200 0.1 sm_100a". */
+const char* bie_version(void);
+/* Number of visible CUDA devices (0 on a machine without a GPU). */
+int bie_device_count(void);
+
+/* ------------------------------------------------------------------------- */
+/* Host-side geometry setup                                                   */
+/* ------------------------------------------------------------------------- */
+/* gausslegendre(n) of FastGaussQuadrature.jl (ascending nodes). Called by the
+ * reference at src/shape/box3d_single.jl:50. */
+int bie_gausslegendre(int n, double* x, double* w);
+/* best_grid_mn (src/utils/best_grid.jl:120-126): m x n tiling with aspect <= alpha. */
+int bie_best_grid(double W, double H, double alpha, int* m, int* n);
+
+typedef struct bie_mesh bie_mesh;
+/* single_dielectric_box3d(Lx, Ly, Lz, n_quad, l_ec, eps_in, eps_out; alpha)
+ * (src/shape/box3d_single.jl:49-70). */
+int bie_mesh_single_box(double Lx, double Ly, double Lz, int n_quad, double l_ec, double eps_in, double eps_out,
+                        double alpha, bie_mesh** out);
+/* multi_dielectric_box3d(n_quad, l_ec, boxes, epses, eps_out; alpha)
+ * (src/shape/box3d_multi.jl:358-386). centers/dims are 3 x nbox. */
+int bie_mesh_multi_box(int n_quad, double l_ec, int nbox, const double* centers, const double* dims,
+                       const double* epses, double eps_out, double alpha, bie_mesh** out);
+/* DielectricInterface of explicit flat panels (rect_panel3d_discretize,
+ * src/shape/box3d.jl:22-64): corners 12 x P (a, b, c, d), normals 3 x P. */
+int bie_mesh_from_panels(int npanels, int n_quad, const double* corners, const double* normals,
+                         const int* is_edge, const double* eps_in, const double* eps_out, bie_mesh** out);
+int bie_mesh_info(const bie_mesh* m, int64_t* npoints, int* npanels, int* n_quad);
+/* Any output pointer may be NULL. pts/nrm are 3 x N, diag is t_P per node
+ * (src/solver/dielectric_box3d.jl:5-15). */
+int bie_mesh_copy(const bie_mesh* m, double* corners, double* normals, int* is_edge, double* eps_in,
+                  double* eps_out, double* pts, double* nrm, double* w, double* diag);
+void bie_mesh_destroy(bie_mesh* m);
+
+/* Near-field correction options; defaults are those of the reference's
+ * corrected operators (src/solver/dielectric_box3d.jl:48-60,
+ * src/solver/multi_rhs.jl:273-275). */
+typedef struct {
+    int max_order;             /* upsampling order cap (default 8) */
+    double up_tol;             /* Bernstein criterion tolerance (default 1e-9) */
+    int correct_edges;         /* include edge panels and touching pairs (default 1) */
+    double adaptive_atol;      /* < 0 => up_tol */
+    double adaptive_rtol;      /* default sqrt(eps) */
+    int adaptive_n_GL;         /* 0 => n_quad */
+    int adaptive_max_depth;    /* default 20 */
+    int nthreads;              /* host threads, 0 = all */
+} bie_near_opts;
+void bie_near_opts_default(bie_near_opts* o);
+
+typedef struct bie_near bie_near;
+/* build_neighbor_list (src/kernel/laplace3d_near.jl:240-392) and
+ * laplace3d_DT_corrections (src/kernel/laplace3d_near_upsampling.jl:127-276),
+ * stored block-sparse: block rows = target panels, blocks nb x nb (nb = n_quad^2),
+ * column-major within a block (val[b*nb*nb + s*nb + r] = C[row r, col s]). */
+int bie_near_build(const bie_mesh* m, const bie_near_opts* o, bie_near** out);
+int bie_near_info(const bie_near* n, int64_t* nblocks, int* nb, int* n_upsample, int* n_adaptive, int* hit_max_depth);
+/* rowptr: npanels + 1, col: nblocks, val: nblocks*nb*nb; pair lists (0-based
+ * source panel i, target panel j, upsampling order p). Any pointer may be NULL. */
+int bie_near_copy(const bie_near* n, int32_t* rowptr, int32_t* col, double* val, int32_t* ups_i, int32_t* ups_j,
+                  int32_t* ups_p, int32_t* adp_i, int32_t* adp_j);
+void bie_near_destroy(bie_near* n);
+
+/* ------------------------------------------------------------------------- */
+/* Device-resident geometry                                                   */
+/* ------------------------------------------------------------------------- */
+typedef struct bie_geom bie_geom;
+/* Copies nodes, normals, weights, diagonal and (optional) BSR correction blocks
+ * to `device`. Replaces the SoA gather of laplace3d_DT_fmm3d
+ * (src/kernel/laplace3d.jl:84-97) and BatchedDielectricOperator's fields
+ * (src/solver/multi_rhs.jl:46-54). bsr_* may be NULL (no corrections). */
+int bie_geom_create(const double* pts, const double* nrm, const double* w, const double* diag, int64_t n,
+                    int32_t npanels, int32_t nb, const int32_t* bsr_rowptr, const int32_t* bsr_col,
+                    const double* bsr_val, int64_t nblocks, int device, bie_geom** out);
+/* Convenience: from a mesh and (optional) near-field blocks. */
+int bie_geom_create_from_mesh(const bie_mesh* m, const bie_near* near, int device, bie_geom** out);
+int bie_geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* device_bytes);
+/* The CUDA stream (cudaStream_t) the handle's work is ordered on. */
+void* bie_geom_stream(bie_geom* g);
+void bie_geom_destroy(bie_geom* g);
+
+/* ------------------------------------------------------------------------- */
+/* Operators                                                                  */
+/* ------------------------------------------------------------------------- */
+/* Y = (D^T + C + diag(t)) X for k columns: the action of lhs_dielectric_box3d
+ * (dense, src/solver/dielectric_box3d.jl:1-17) and of
+ * lhs_dielectric_box3d_fmm3d_corrected / BatchedDielectricOperator mul!
+ * (src/solver/dielectric_box3d.jl:48-92, src/solver/multi_rhs.jl:103-136) with the
+ * FMM replaced by the exact direct sum (j != i). Host arrays, N x k column-major. */
+int bie_matvec(bie_geom* g, const double* X, double* Y, int32_t k, int32_t precision, uint32_t flags);
+/* Same on device arrays (node-major N x k) ordered on `stream` (NULL = the handle's). */
+int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int32_t precision, uint32_t flags,
+                      void* stream);
+
+/* F[:, c] = rhs_dielectric_box3d(itf, PointSource(src[:, c], q[c]), eps_src[c])
+ * (src/solver/dielectric_box3d.jl:95-104). src 3 x k, F N x k (host). */
+int bie_rhs_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* F);
+int bie_rhs_point_device(bie_geom* g, const double* d_src, const double* d_q, const double* d_eps_src, int32_t k,
+                         double* dF, void* stream);
+
+/* phi[m, c] = S[Sigma[:, c]](targets[:, m]) = sum_j w_j Sigma[j, c] / (4 pi |x_m - y_j|)
+ * (laplace3d_pottrg, src/kernel/laplace3d.jl:69-82). targets 3 x M, phi M x k (host). */
+int bie_potential(bie_geom* g, const double* Sigma, int32_t k, const double* targets, int64_t M, double* phi);
+/* Same with device arrays: d_sigma node-major N x k, d_targets 3 x M, d_phi M x k row-major. */
+int bie_potential_device(bie_geom* g, const double* d_sigma, int32_t k, const double* d_targets, int64_t M,
+                         double* d_phi, void* stream);
+/* Polarisation energy of point sources: W[c] = 1/2 q[c] S[Sigma[:, c]](src[:, c]). src 3 x k. */
+int bie_energy(bie_geom* g, const double* Sigma, int32_t k, const double* src, const double* q, double* W);
+
+/* ------------------------------------------------------------------------- */
+/* Solvers                                                                    */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    double atol;         /* absolute residual tolerance (default 0) */
+    double rtol;         /* relative residual tolerance per column (default 1e-10) */
+    int itmax;           /* maximum Krylov iterations in total (default 500) */
+    int restart;         /* Krylov basis capacity before restart (default 200) */
+    int precision;       /* bie_precision of the Krylov operator (default BIE_FP64) */
+    double inner_rtol;   /* mixed precision: relative tolerance of each inner solve (default 1e-5) */
+    int max_outer;       /* mixed precision: maximum refinement steps (default 8) */
+    int precondition;    /* right diagonal preconditioner 1/t_P (src/solver/multi_rhs.jl:234-247) */
+    int check_every;     /* host convergence check period in iterations (default 1) */
+    uint32_t flags;      /* BIE_NO_CORRECTIONS etc. applied to the operator */
+} bie_solve_opts;
+void bie_solve_opts_default(bie_solve_opts* o);
+
+typedef struct {
+    int iterations;       /* Krylov iterations (all refinement steps) */
+    int outer;            /* refinement steps (1 for FP64) */
+    int fp64_matvecs;     /* full FP64 operator applications */
+    int lowp_matvecs;     /* reduced-precision operator applications */
+    int converged;        /* all columns reached atol + rtol * ||F[:, c]|| */
+    double max_rel_resid; /* max_c ||F - A Sigma||_c / ||F||_c, FP64 true residual */
+    double seconds;       /* device time of the solve */
+    int* col_iterations;  /* optional (k entries): Krylov iterations per column */
+    double* col_resid;    /* optional (k entries): final true relative residual per column */
+} bie_stats;
+
+/* Solves (D^T + C + diag(t)) Sigma = F for k right-hand sides: solve_gmres /
+ * Krylov.gmres (src/utils/linear_algebra.jl:3-5) for k = 1 and
+ * solve_dielectric_box3d_block / Krylov.block_gmres (src/solver/multi_rhs.jl:270-286)
+ * for k > 1, run on the device (all k columns iterate together, each with its own
+ * Arnoldi process; converged columns are frozen). With precision != BIE_FP64 the
+ * Krylov operator is the reduced-precision one inside FP64 iterative refinement.
+ * Host arrays N x k. Returns BIE_ENOCONV (with Sigma filled) when itmax is hit. */
+int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st);
+int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o,
+                     bie_stats* st, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BIE_B200_H */
