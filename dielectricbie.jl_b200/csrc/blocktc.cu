@@ -1,0 +1,441 @@
+// K3: block direct sum for k >= 16 right-hand sides on the 5th-generation tensor
+// cores (tcgen05, sm_100a).
+//
+//   part[s][i][c0 + c] = sum_{j in split s, j != i} G(i, j) Q(j, c)
+//   G(i, j) = n_i . (x_i - y_j) / |x_i - y_j|^3        (generated in FP32 registers)
+//   Q(j, c) = w_j p_j X[j][c0 + c]                     (packed per call)
+//
+// G is the adjoint double-layer kernel of laplace3d_DT (src/kernel/laplace3d.jl:30-40);
+// the contraction replaces the batched lfmm3d(nd = K) of
+// mul!(Y, ::BatchedDielectricOperator, X) (src/solver/multi_rhs.jl:103-130).
+//
+// Split-BF16 three-term product: with G = Gh + Gl and Q = Qh + Ql (bf16 hi/lo),
+// G Q ~= Gh Qh + Gh Ql + Gl Qh (the dropped Gl Ql term is ~2^-16 relative),
+// accumulated in FP32 in tensor memory; each source split writes an FP64 partial.
+//
+// CTA = 192 threads: warps 0-3 generate the 128 x 64 kernel tile of a source
+// chunk (one thread per target row, K-major rows in the 128-byte swizzled
+// layout the UMMA descriptors read) and run the epilogue; warp 4 issues the
+// MMAs (one thread); warp 5 streams the pre-swizzled Q tiles with bulk copies.
+// Every mbarrier wait is bounded: on expiry the CTA records an error code and
+// returns after releasing its tensor memory.
+#include <cuda_bf16.h>
+#include <algorithm>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "solver.h"
+
+namespace bie {
+namespace tc {
+
+constexpr int M = 128;      // targets per tile (MMA M)
+constexpr int KC = 64;      // sources per chunk = one 128-byte bf16 row
+constexpr int S = 2;        // pipeline stages
+constexpr int NTHREADS = 192;
+constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr int kErrTimeout = 1;
+
+struct Params {
+    GeomDev g;
+    const uint8_t* bpack;  // [nchunks][2][npad][128 B] pre-swizzled bf16 images (hi, lo)
+    int npad;              // MMA N (multiple of 16, <= 256)
+    int keff;              // columns stored (<= npad)
+    int64_t nchunks;
+    int64_t cps;           // chunks per split
+    double* part;          // [nsplit][n][ldp]
+    int ldp, c0;
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait; returns false (and flags the CTA) when the limit expires.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        if (mbar_try(b, parity)) return true;
+        if (*abort_flag) return false;
+    }
+    *abort_flag = 1;
+    return false;
+}
+
+// Wait bounded by an iteration limit only (used to drain in-flight work on the abort path).
+__device__ __forceinline__ bool mbar_wait_raw(uint64_t* b, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try(b, parity)) return true;
+    return false;
+}
+
+// OR-reduction of a predicate over the 128 generator threads (named barrier 1):
+// also orders their shared-memory accesses like bar.sync.
+__device__ __forceinline__ bool gen_any(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, 128, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    // K-major, 128-byte swizzle: rows of 128 B, 8-row atoms 1024 B apart (SBO),
+    // LBO unused (1), descriptor version 1, layout type 2 (SWIZZLE_128B).
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+
+__device__ __forceinline__ uint32_t idesc_bf16(int n) {
+    // c_format F32 (1) @4, a/b format BF16 (1) @7/@10, K-major A/B, N>>3 @17, M>>4 @24
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo_elem, hi_elem);  // .x (low 16 bits) = lo_elem
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// Split two FP32 values into packed bf16 hi and lo words.
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+    hi = pack_bf16(a, b);
+    float ah = __uint_as_float(hi << 16), bh = __uint_as_float(hi & 0xFFFF0000u);
+    lo = pack_bf16(a - ah, b - bh);
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // carve-up aligned to 1024 bytes in the shared window (128-byte swizzle atoms)
+    uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const int npad = P.npad;
+    const uint32_t a_bytes = M * 128;          // one term of the A tile (16 KB)
+    const uint32_t b_bytes = (uint32_t)npad * 128;  // one term of the B tile
+    uint8_t* A = base;                               // [S][2][a_bytes]
+    uint8_t* B = A + S * 2 * a_bytes;                // [S][2][b_bytes]
+    float4* crd = (float4*)(B + S * 2 * b_bytes);    // [S][KC]
+    uint64_t* full_a = (uint64_t*)(crd + S * KC);
+    uint64_t* full_b = full_a + S;
+    uint64_t* empty = full_b + S;
+    uint64_t* acc_done = empty + S;
+    uint32_t* tmem_slot = (uint32_t*)(acc_done + 1);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t n = P.g.n;
+    const int64_t i0 = (int64_t)blockIdx.x * M;
+    const int64_t ch0 = (int64_t)blockIdx.y * P.cps;
+    const int64_t ch1 = min(P.nchunks, ch0 + P.cps);
+    const int nch = ch1 > ch0 ? (int)(ch1 - ch0) : 0;
+    const uint32_t tcols = npad <= 32 ? 32 : (npad <= 64 ? 64 : (npad <= 128 ? 128 : 256));
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full_a[s], 128);
+            mbar_init(&full_b[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(tcols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    // tile origin: coordinates are rounded to FP32 relative to it
+    const int64_t io = min(i0, n - 1);
+    const double ox = P.g.x[io], oy = P.g.y[io], oz = P.g.z[io];
+
+    if (warp < 4) {
+        // ------------------------- generators -------------------------------
+        const int r = threadIdx.x;  // tile row
+        const int64_t i = i0 + r;
+        const bool valid = i < n;
+        float xi, yi, zi, n0, n1, n2;
+        if (valid) {
+            xi = (float)(P.g.x[i] - ox); yi = (float)(P.g.y[i] - oy); zi = (float)(P.g.z[i] - oz);
+            n0 = (float)P.g.nx[i]; n1 = (float)P.g.ny[i]; n2 = (float)P.g.nz[i];
+        } else {
+            xi = yi = zi = -1.0e18f;  // far from every node and every padded source: G underflows to 0
+            n0 = n1 = n2 = 0.f;
+        }
+        const uint32_t row_off = (uint32_t)r * 128u;
+        const uint32_t rsw = (uint32_t)(r & 7);
+        for (int lc = 0; lc < nch; ++lc) {
+            const int s = lc % S;
+            const uint32_t u = (uint32_t)(lc / S);
+            const int64_t j0 = (ch0 + lc) * KC;
+            if (threadIdx.x < KC) {
+                const int64_t j = j0 + threadIdx.x;
+                float4 c;
+                if (j < n)
+                    c = make_float4((float)(P.g.x[j] - ox), (float)(P.g.y[j] - oy), (float)(P.g.z[j] - oz), 0.f);
+                else
+                    c = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.f);  // padded source: G underflows to 0
+                crd[s * KC + threadIdx.x] = c;
+            }
+            bool fail = (lc >= S) && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag);
+            if (gen_any(fail)) break;  // uniform exit; the barrier also publishes crd[s]
+            uint8_t* Ah = A + (s * 2 + 0) * a_bytes;
+            uint8_t* Al = A + (s * 2 + 1) * a_bytes;
+            const float4* cs = crd + s * KC;
+            const bool self = (j0 < i0 + M) && (j0 + KC > i0);
+#pragma unroll 1
+            for (int gq = 0; gq < KC / 8; ++gq) {
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const float4 c = cs[gq * 8 + e];
+                    float dx = xi - c.x, dy = yi - c.y, dz = zi - c.z;
+                    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    float ri = rsqrtf(r2);
+                    float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+                    v[e] = nd * (ri * ri * ri);
+                }
+                if (self) {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        if (j0 + gq * 8 + e == i) v[e] = 0.f;
+                }
+                uint4 h, l;
+                split2(v[0], v[1], h.x, l.x);
+                split2(v[2], v[3], h.y, l.y);
+                split2(v[4], v[5], h.z, l.z);
+                split2(v[6], v[7], h.w, l.w);
+                const uint32_t off = row_off + ((((uint32_t)gq) ^ rsw) << 4);
+                *reinterpret_cast<uint4*>(Ah + off) = h;
+                *reinterpret_cast<uint4*>(Al + off) = l;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&full_a[s]);
+        }
+        // ------------------------- epilogue ---------------------------------
+        bool ok = !*abort_flag;
+        if (nch > 0 && ok) ok = mbar_wait(acc_done, 0, abort_flag);
+        ok = !gen_any(!ok);  // every generator warp takes the same branch
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (ok) {
+            const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+            double* out = P.part + ((int64_t)blockIdx.y * n + i) * P.ldp + P.c0;
+            for (int c = 0; c < npad; c += 16) {
+                float v[16];
+                if (nch > 0) {
+                    tmem_ld16(tmem + lane_base + (uint32_t)c, v);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) v[q] = 0.f;
+                }
+                if (valid) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (c + q < P.keff) out[c + q] = (double)v[q];
+                }
+            }
+        }
+    } else if (warp == 4) {
+        // ------------------------- MMA issuer --------------------------------
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16(npad);
+            for (int lc = 0; lc < nch; ++lc) {
+                const int s = lc % S;
+                const uint32_t u = (uint32_t)(lc / S);
+                if (!mbar_wait(&full_a[s], u & 1, abort_flag)) break;
+                if (!mbar_wait(&full_b[s], u & 1, abort_flag)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t ah = smem_u32(A + (s * 2 + 0) * a_bytes), al = smem_u32(A + (s * 2 + 1) * a_bytes);
+                const uint32_t bh = smem_u32(B + (s * 2 + 0) * b_bytes), bl = smem_u32(B + (s * 2 + 1) * b_bytes);
+#pragma unroll
+                for (int kk = 0; kk < KC / 16; ++kk) {
+                    const uint32_t ko = (uint32_t)kk * 32u;
+                    mma_bf16(tmem, sw128_desc(ah + ko), sw128_desc(bh + ko), idesc, (lc > 0 || kk > 0) ? 1u : 0u);
+                    mma_bf16(tmem, sw128_desc(ah + ko), sw128_desc(bl + ko), idesc, 1u);
+                    mma_bf16(tmem, sw128_desc(al + ko), sw128_desc(bh + ko), idesc, 1u);
+                }
+                mma_commit(&empty[s]);
+            }
+            mma_commit(acc_done);
+            // on abort, drain this thread's MMAs before the CTA releases tensor memory
+            if (*abort_flag) mbar_wait_raw(acc_done, 0);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------- Q-tile producer ---------------------------
+        if (lane == 0) {
+            const uint32_t bytes = 2 * b_bytes;
+            int issued = 0;
+            for (int lc = 0; lc < nch; ++lc) {
+                const int s = lc % S;
+                const uint32_t u = (uint32_t)(lc / S);
+                if (lc >= S && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag)) break;
+                mbar_arrive_tx(&full_b[s], bytes);
+                bulk_g2s(B + s * 2 * b_bytes, P.bpack + (size_t)(ch0 + lc) * bytes, bytes, &full_b[s]);
+                issued = lc + 1;
+            }
+            // on abort, wait for the copies still in flight (at most one per stage)
+            if (*abort_flag)
+                for (int lc = issued > S ? issued - S : 0; lc < issued; ++lc) mbar_wait_raw(&full_b[lc % S], (lc / S) & 1);
+        }
+        __syncwarp();
+    }
+
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*abort_flag && threadIdx.x == 0) atomicOr(P.err, kErrTimeout);
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols) : "memory");
+    }
+}
+
+// Packs Q(j, c) = w_j p_j X[j][c0 + c] as bf16 hi/lo, in the swizzled K-major
+// smem image of each 64-source chunk: [chunk][term][row c][128 B]. Rows c >= keff
+// and sources j >= n are zero.
+__global__ void k_pack_q(GeomDev g, const double* __restrict__ X, int ldx, int c0, int keff,
+                         const double* __restrict__ pre, int npad, int64_t nchunks, uint8_t* __restrict__ out) {
+    // one thread per (chunk, row c, 8-source group)
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = nchunks * npad * 8;
+    if (e >= total) return;
+    const int gq = (int)(e & 7);
+    const int c = (int)((e >> 3) % npad);
+    const int64_t ch = (e >> 3) / npad;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int64_t j = ch * KC + gq * 8 + q;
+        double val = 0.0;
+        if (j < g.n && c < keff) val = g.w[j] * (pre ? pre[j] : 1.0) * X[j * ldx + c0 + c];
+        v[q] = (float)val;
+    }
+    uint4 h, l;
+    split2(v[0], v[1], h.x, l.x);
+    split2(v[2], v[3], h.y, l.y);
+    split2(v[4], v[5], h.z, l.z);
+    split2(v[6], v[7], h.w, l.w);
+    const size_t tile = (size_t)npad * 128;
+    uint8_t* base = out + (size_t)ch * 2 * tile;
+    const uint32_t off = (uint32_t)c * 128u + ((((uint32_t)gq) ^ (uint32_t)(c & 7)) << 4);
+    *reinterpret_cast<uint4*>(base + off) = h;
+    *reinterpret_cast<uint4*>(base + tile + off) = l;
+}
+
+size_t smem_bytes(int npad) {
+    size_t a = (size_t)S * 2 * M * 128, b = (size_t)S * 2 * npad * 128;
+    size_t c = (size_t)S * KC * sizeof(float4);
+    size_t bars = (3 * S + 1) * sizeof(uint64_t) + 16;
+    return 1024 + a + b + c + bars;
+}
+
+}  // namespace tc
+
+int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
+
+// Runs K3 for columns [c0, c0 + kc) (kc <= 256) of X into part[s][i][c0 + c].
+void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
+                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s) {
+    const int npad = tc_npad(kc);
+    const int64_t nchunks = (g.n + tc::KC - 1) / tc::KC;
+    const int64_t pk = nchunks * npad * 8;
+    tc::k_pack_q<<<(unsigned)((pk + 255) / 256), 256, 0, s>>>(g, X, ldx, c0, kc, pre, npad, nchunks, bpack);
+    BIE_CK(cudaGetLastError());
+    tc::Params P;
+    P.g = g;
+    P.bpack = bpack;
+    P.npad = npad;
+    P.keff = kc;
+    P.nchunks = nchunks;
+    P.cps = cps;
+    P.part = part;
+    P.ldp = ldp;
+    P.c0 = c0;
+    P.err = err;
+    const size_t sm = tc::smem_bytes(npad);
+    static size_t configured = 0;
+    if (sm > configured) {
+        BIE_CK(cudaFuncSetAttribute(tc::k_dt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        configured = sm;
+    }
+    dim3 grid((unsigned)((g.n + tc::M - 1) / tc::M), (unsigned)nsplit);
+    tc::k_dt_tc<<<grid, tc::NTHREADS, sm, s>>>(P);
+    BIE_CK(cudaGetLastError());
+}
+
+size_t block_tc_pack_bytes(int64_t n, int kc) {
+    const int64_t nchunks = (n + tc::KC - 1) / tc::KC;
+    return (size_t)nchunks * 2 * tc_npad(kc) * 128;
+}
+
+int block_tc_ctas_per_sm(int kc) {
+    const size_t sm = tc::smem_bytes(tc_npad(kc));
+    return std::max(1, (int)((227 * 1024) / (sm + 1024)));
+}
+
+}  // namespace bie

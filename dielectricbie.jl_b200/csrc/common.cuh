@@ -1,0 +1,29 @@
+// Device-side types shared by the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bie {
+
+constexpr double kInv4Pi = 0.079577471545947667884;  // 1 / (4 pi)
+constexpr int kTB = 128;  // targets per CTA of the direct-sum kernels (one per thread)
+constexpr int kTS = 128;  // sources per shared-memory tile
+
+// Device-resident geometry: SoA FP64 arrays of length n.
+struct GeomDev {
+    const double *x, *y, *z;     // node positions
+    const double *nx, *ny, *nz;  // node normals
+    const double* w;             // quadrature weights
+    int64_t n;
+};
+
+// K3 (blocktc.cu): tensor-core block direct sum for columns [c0, c0 + kc), kc <= 256.
+void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
+                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s);
+size_t block_tc_pack_bytes(int64_t n, int kc);
+int block_tc_ctas_per_sm(int kc);
+int tc_npad(int kc);
+constexpr int kTcTileM = 128;   // targets per tensor-core tile
+constexpr int kTcChunk = 64;    // sources per tensor-core chunk
+
+}  // namespace bie

@@ -9,18 +9,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "common.cuh"
+
 namespace bie {
-
-constexpr double kInv4Pi = 0.079577471545947667884;  // 1 / (4 pi)
-constexpr int kTB = 128;  // targets per CTA of the direct-sum kernels (one per thread)
-constexpr int kTS = 128;  // sources per shared-memory tile
-
-struct GeomDev {
-    const double *x, *y, *z;     // node positions
-    const double *nx, *ny, *nz;  // node normals
-    const double* w;             // quadrature weights
-    int64_t n;
-};
 
 // ---------------------------------------------------------------------------
 // K1: FP64 direct D^T sum ("plain").  part[s][i][c0 + c] =

@@ -22,7 +22,7 @@ struct bie_geom {
     bie::Buf x, y, z, nx, ny, nz, w, diag, pinv;
     bie::Buf rowptr, col, val;
     // operator workspace
-    bie::Buf part, small;
+    bie::Buf part, small, bpack, errflag;
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -166,14 +166,43 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
     return sp;
 }
 
+// K3 launch plan: enough source splits for >= 2 waves of CTAs, and at most 256
+// chunks (16384 sources) accumulated in FP32 tensor memory per FP64 partial.
+Split tc_split(const bie_geom* g, int kc) {
+    const int64_t tiles = (g->n + kTcTileM - 1) / kTcTileM;
+    const int64_t chunks = (g->n + kTcChunk - 1) / kTcChunk;
+    const int64_t slots = (int64_t)g->sms * block_tc_ctas_per_sm(kc);
+    int64_t ns = std::max<int64_t>(1, (2 * slots + tiles - 1) / tiles);
+    ns = std::max<int64_t>(ns, (chunks + 255) / 256);
+    ns = std::min<int64_t>(ns, chunks);
+    int64_t cps = (chunks + ns - 1) / ns;
+    ns = (chunks + cps - 1) / cps;
+    return Split{(int)ns, cps};
+}
+
+Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, cudaStream_t s) {
+    GeomDev gd = gdev(g);
+    Split sp = tc_split(g, std::min(k, 256));
+    g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
+    g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 256)));
+    for (int c0 = 0; c0 < k; c0 += 256) {
+        int kc = std::min(256, k - c0);
+        launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, g->bpack.as<uint8_t>(),
+                        g->errflag.as<int>(), s);
+    }
+    return sp;
+}
+
 // Y = A(prec) (p .* X), node-major n x k (ldx = ldy = k).
 void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
               cudaStream_t s) {
-    Kern kind;
-    if (prec == BIE_FP64) kind = Kern::DT64;
-    else if (prec == BIE_FP32) kind = Kern::DT32;
-    else throw Error(BIE_EUNSUPPORTED, "precision BIE_BF16X3 is not available in this build");
-    Split sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
+    Split sp;
+    if (prec == BIE_BF16X3 && k >= 16) {
+        sp = direct_sum_tc(g, X, k, pre, s);
+    } else {
+        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // BF16X3 with k < 16 runs the FP32 kernel
+        sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
+    }
     const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
     const bool dg = !(flags & BIE_NO_DIAG);
     k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
@@ -350,6 +379,17 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
     return res;
 }
 
+// Raises BIE_ETIMEOUT if a kernel recorded an expired bounded wait (and clears the flag).
+void check_device_error(bie_geom* g, cudaStream_t s) {
+    int e = 0;
+    BIE_CK(cudaMemcpyAsync(&e, g->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+    if (e) {
+        BIE_CK(cudaMemsetAsync(g->errflag.p, 0, sizeof(int), s));
+        throw Error(BIE_ETIMEOUT, "a device wait ran out of its iteration limit (kernel returned early)");
+    }
+}
+
 void check_prec(int prec) {
     if (prec != BIE_FP64 && prec != BIE_FP32 && prec != BIE_BF16X3) throw Error(BIE_EINVAL, "unknown precision");
 }
@@ -393,6 +433,8 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
     }
     upload(g->w, w, n, s);
     upload(g->diag, diag, n, s);
+    g->errflag.ensure(sizeof(int));
+    BIE_CK(cudaMemsetAsync(g->errflag.p, 0, sizeof(int), s));
     for (int64_t i = 0; i < n; ++i) col3[i] = diag[i] != 0.0 ? 1.0 / diag[i] : 1.0;
     upload(g->pinv, col3.data(), n, s);
     if (nblocks > 0) {
@@ -412,7 +454,7 @@ void geom_destroy(bie_geom* g) {
         DeviceGuard dg(g->device);
         if (g->stream) cudaStreamSynchronize(g->stream);
         bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->rowptr,
-                           &g->col, &g->val, &g->part, &g->small, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
+                           &g->col, &g->val, &g->part, &g->small, &g->bpack, &g->errflag, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
                            &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
         for (auto* b : all) b->release();
@@ -456,6 +498,7 @@ void matvec_host(bie_geom* g, const double* X, double* Y, int k, int precision, 
     BIE_CK(cudaGetLastError());
     BIE_CK(cudaMemcpyAsync(Y, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));
+    check_device_error(g, s);
 }
 
 void rhs_point_device(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* F,
@@ -609,6 +652,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
     }
     BIE_CK(cudaEventRecord(g->ev1, s));
     BIE_CK(cudaEventSynchronize(g->ev1));
+    check_device_error(g, s);
     float ms = 0.f;
     BIE_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
     if (st) {

@@ -146,3 +146,32 @@ def test_potential_and_energy(bie, orc, cfg1, rng):
     for c, s in enumerate(src):
         ref_c = 0.5 * s.charge * orc.pottrg_apply(m.pts, m.w, np.array([s.point]), S[:, c])[0]
         assert abs(W[c] - ref_c) <= 1e-13 * abs(ref_c)
+
+
+@pytest.mark.parametrize("k", [16, 20, 64])
+def test_matvec_bf16x3_tensor_core(bie, cfg1, rng, k):
+    """K3 (tcgen05 split-BF16 three-term contraction) vs the FP64 operator: the dropped
+    lo*lo term and FP32 accumulation bound the error near 1e-5 relative."""
+    itf = cfg1[0]
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-9, 1e-9, 8)
+    X = rng.standard_normal((itf.n, k))
+    Y64 = op.mul(X)
+    Ytc = op.mul(X, precision="bf16x3")
+    for c in range(k):
+        assert rel(Ytc[:, c], Y64[:, c]) < 5e-5, (c, rel(Ytc[:, c], Y64[:, c]))
+    # self-interaction excluded, corrections and diagonal intact: near the FP32 operator
+    assert rel(Ytc, op.mul(X, precision="fp32")) < 5e-5
+
+
+def test_solve_refined_bf16x3_vs_lu(bie, orc, cfg1, rng):
+    itf, m, Cm, A = cfg1
+    Ac = A + Cm.toarray()
+    src = rng.uniform(-0.25, 0.25, (16, 3))
+    q = rng.standard_normal(16)
+    B = np.stack([orc.rhs_point(m.pts, m.nrm, s, qq, 4.0) for s, qq in zip(src, q)], axis=1)
+    X_lu = sla.lu_solve(sla.lu_factor(Ac), B)
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, 1e-9, 8, precision="bf16x3")
+    X, st = bie.gpu_solve(op, B, rtol=1e-11, itmax=400)
+    assert st.solved and st.lowp_matvecs > 0
+    for c in range(16):
+        assert rel(X[:, c], X_lu[:, c]) < 1e-8
