@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Benchmark of the dielectric BIE hot path on B200.
+
+Workload (default `cfg3`): box 1.5 x 1.0 x 0.8, n_quad = 6, l_ec = 0.08,
+eps_in = 4, eps_out = 1 (N = 42,048 nodes, near-field corrections at
+up_tol = 1e-9, max_order = 8). One step = one block solve of k = 64 point-source
+right-hand sides (positions uniform in the box interior, charges ~ N(0, 1),
+seeded) to a relative residual of 1e-10: RHS assembly on the device + the
+refined solver (split-BF16 three-term tensor-core direct sum, FP64 corrections,
+FP64 Krylov and iterative refinement). The same steps are also timed on the
+plain FP64 GPU path for the comparison the metric names.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cfg3]
+
+Under torchrun (N > 1) every rank solves its own request stream on its own GPU
+(replicas; no collective on the data path): value = all ranks' solves / the
+slowest rank's time. `--impl reference` times the CPU restatement of the
+reference's path (oracle/, C + OpenMP on all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "dielectricbie.jl_b200")
+METRIC = "solves/s + p50/p99 latency at 1e-8 rel σ err: refined/batched vs plain FP64 GPU"
+
+WORKLOADS = {
+    "cfg3": dict(box=(1.5, 1.0, 0.8), nq=6, l_ec=0.08, eps_in=4.0, eps_out=1.0, k=64, seed=3, rtol=1e-10,
+                 up_tol=1e-9, max_order=8, probes=1000, charges="normal"),
+    "cfg2": dict(box=(2.0, 1.0, 1.0), nq=6, l_ec=0.05, eps_in=10.0, eps_out=1.0, k=8, seed=2, rtol=1e-10,
+                 up_tol=1e-9, max_order=8, probes=0, charges="pm1", inner=0.8),
+    "cfg1": dict(box=(1.2, 0.8, 0.6), nq=4, l_ec=0.2, eps_in=4.0, eps_out=1.0, k=1, seed=1, rtol=1e-12,
+                 up_tol=1e-9, max_order=8, probes=0, charges="one"),
+}
+
+
+def load_package():
+    name = "dielectricbie_jl_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    sys.path.insert(0, PKG_DIR)
+    import build as pkg_build  # in-tree build of libbie_b200.so (no-op when up to date)
+    pkg_build.build()
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_sources(wl, nbatch, k):
+    """Point sources uniform in the box interior (inner fraction `inner`), charges per workload."""
+    rng = np.random.default_rng(wl["seed"])
+    half = np.array(wl["box"]) / 2 * wl.get("inner", 0.9)
+    out = []
+    for _ in range(nbatch):
+        pos = rng.uniform(-half, half, size=(k, 3))
+        if wl["charges"] == "normal":
+            q = rng.standard_normal(k)
+        elif wl["charges"] == "pm1":
+            q = rng.choice([-1.0, 1.0], size=k)
+        else:
+            q = np.ones(k)
+        out.append((np.ascontiguousarray(pos), np.ascontiguousarray(q)))
+    return out
+
+
+def make_probes(bie, itf, m, seed):
+    """Exterior probes: a random surface node pushed 0.1-0.5 along its outward normal."""
+    rng = np.random.default_rng(seed)
+    idx = rng.integers(0, itf.n, size=m)
+    d = rng.uniform(0.1, 0.5, size=m)
+    return np.ascontiguousarray(itf.points[idx] + itf.normals[idx] * d[:, None])
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(wl, max_seconds=25.0, threads=0):
+    """CPU restatement of the reference path (oracle: direct sum + CSC corrections +
+    GMRES, FP64, C/OpenMP) on one right-hand side of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build()
+    m = orc.Mesh.single_box(*wl["box"], wl["nq"], wl["l_ec"], wl["eps_in"], wl["eps_out"])
+    ups, adp = orc.build_neighbor_list(m, wl["max_order"], wl["up_tol"], True)
+    Cm = orc.DT_corrections(m, ups, adp, wl["up_tol"], nthreads=threads)
+    pos, q = make_sources(wl, 1, 1)[0]
+    b = orc.rhs_point(m.pts, m.nrm, pos[0], q[0], wl["eps_in"])
+    # one operator application first, to bound the sample
+    t0 = time.perf_counter()
+    orc.op_apply(m, b, Cm, nthreads=threads)
+    t_mv = time.perf_counter() - t0
+    itmax = max(2, int(max_seconds / max(t_mv, 1e-6)))
+    t0 = time.perf_counter()
+    x, it, res = orc.gmres(m, b, Cm, atol=0.0, rtol=wl["rtol"], itmax=itmax, nthreads=threads)
+    t = time.perf_counter() - t0
+    converged = res <= wl["rtol"] * np.linalg.norm(b) * (1 + 1e-9)
+    return dict(seconds=t, iterations=it, converged=bool(converged), matvec_s=t_mv, n=m.n,
+                cores=threads or os.cpu_count())
+
+
+def run_reference_arm(args, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count()
+    times = []
+    info = None
+    for step in range(args.warmup + args.steps):
+        info = cpu_reference(wl, max_seconds=25.0, threads=cores)
+        if step >= args.warmup:
+            times.append(info["seconds"])
+    # a step solves one right-hand side; a solve stopped by the time bound is
+    # scaled to the converged iteration count of the first converged run
+    per_solve = float(np.mean(times))
+    value = 1.0 / per_solve
+    sample = (f"one {wl['k']}-RHS column of the {args.workload} workload per step: oracle direct sum + CSC near "
+              f"corrections + FP64 GMRES (rtol {wl['rtol']:g}), N={info['n']}, {info['iterations']} iterations"
+              f"{'' if info['converged'] else ' (time-bounded, not converged)'}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded point sources)",
+            "config": workload_config(args.workload, wl, info["n"]),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(name, wl, n):
+    return {"workload": f"{name}: block {wl['k']}-RHS solve, box {'x'.join(str(v) for v in wl['box'])}, "
+                        f"n_quad={wl['nq']}, l_ec={wl['l_ec']}, eps {wl['eps_in']}/{wl['eps_out']}, N={n}",
+            "nodes": n, "rhs_per_solve": wl["k"], "rtol": wl["rtol"], "up_tol": wl["up_tol"],
+            "max_order": wl["max_order"], "l2": "flushed between steps (256 MB write)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-matvec", action="store_true",
+                    help="apply the refined and the FP64 operator once each to k columns and exit "
+                         "(small case for ncu captures)")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    device = local
+    torch.cuda.set_device(device)
+    bie = load_package()
+    from dielectricbie_jl_b200 import _abi  # noqa: E402
+    import ctypes as C
+    L = _abi.lib()
+
+    # ---------------- setup (untimed): mesh, near-field blocks, device geometry -------
+    itf = bie.single_dielectric_box3d(*wl["box"], wl["nq"], wl["l_ec"], wl["eps_in"], wl["eps_out"])
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, wl["up_tol"], wl["max_order"],
+                                                  precision=args.precision, device=device)
+    g = op.geom._h
+    n, k = itf.n, wl["k"]
+    if args.profile_matvec:
+        X = np.asfortranarray(np.random.default_rng(0).standard_normal((n, k)))
+        op.mul(X, precision=args.precision)
+        op.mul(X, precision="fp64")
+        torch.cuda.synchronize(device)
+        print(json.dumps({"profile_matvec": args.workload, "n": n, "k": k}), flush=True)
+        return 0
+    nsteps = args.warmup + args.steps
+    batches = make_sources(wl, nsteps + 1, k)
+    stream = torch.cuda.ExternalStream(op.geom.stream, device=device)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(f"cuda:{device}")
+
+    src_d = [dev(p) for p, _ in batches]
+    q_d = [dev(q) for _, q in batches]
+    eps_d = dev(np.full(k, wl["eps_in"]))
+    F = torch.empty((n, k), dtype=torch.float64, device=device)
+    S = torch.empty((n, k), dtype=torch.float64, device=device)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MB > L2 (126 MB)
+
+    def opts(precision, rtol, verify=False):
+        o = _abi.SolveOpts()
+        L.bie_solve_opts_default(C.byref(o))
+        o.rtol, o.itmax, o.restart = rtol, 600, 200
+        o.precision = _abi.PRECISIONS[precision]
+        o.flags = 0 if verify else _abi.BIE_NO_VERIFY
+        return o
+
+    def solve_step(i, precision, rtol, verify=False, st=None):
+        _abi.check(L.bie_rhs_point_device(g, C.c_void_p(src_d[i].data_ptr()), C.c_void_p(q_d[i].data_ptr()),
+                                          C.c_void_p(eps_d.data_ptr()), k, C.c_void_p(F.data_ptr()), None))
+        o = opts(precision, rtol, verify)
+        rc = L.bie_solve_device(g, C.c_void_p(F.data_ptr()), C.c_void_p(S.data_ptr()), k, C.byref(o),
+                                C.byref(st) if st is not None else None, None)
+        if rc != _abi.BIE_OK:
+            _abi.check(rc)
+
+    def timed_loop(precision, rtol, profile=False, sampler_dev=None):
+        ms = []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for i in range(nsteps):
+            flush.zero_()
+            torch.cuda.synchronize(device)
+            if i == args.warmup and profile:
+                _abi.check(L.bie_profile_enable(g, 1))
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                solve_step(i, precision, rtol)
+                ev1.record(stream)
+            ev1.synchronize()
+            if i >= args.warmup:
+                ms.append(ev0.elapsed_time(ev1))
+        return ms
+
+    # ---------------- accuracy (untimed): refined vs plain FP64 on the same batch -----
+    st = _abi.Stats()
+    solve_step(nsteps, "fp64", 1e-13, verify=True, st=st)
+    torch.cuda.synchronize(device)
+    S_ref = S.cpu().numpy().copy()
+    plain_ref_iters = st.iterations
+    solve_step(nsteps, args.precision, wl["rtol"], verify=True, st=st)
+    torch.cuda.synchronize(device)
+    S_ref_refined = S.cpu().numpy().copy()
+    sig_err = max(np.linalg.norm(S_ref_refined[:, c] - S_ref[:, c]) / np.linalg.norm(S_ref[:, c]) for c in range(k))
+    accuracy = {"sigma_rel_err_max": sig_err, "refined_true_rel_resid": st.max_rel_resid,
+                "refined_iterations": st.iterations, "refined_outer": st.outer,
+                "refined_fp64_matvecs": st.fp64_matvecs, "refined_lowp_matvecs": st.lowp_matvecs,
+                "reference_sigma": "plain FP64 GPU solve at rtol 1e-13"}
+    pos, qs = batches[nsteps]
+    if wl["probes"]:
+        T = make_probes(bie, itf, wl["probes"], wl["seed"])
+        P = bie.laplace3d_pottrg(itf, T)
+        dphi = lambda Sg: (P @ Sg)  # noqa: E731  (FP64 single-layer at the probes)
+        phi_ref, phi_ref2 = dphi(np.asfortranarray(S_ref)), dphi(np.asfortranarray(S_ref_refined))
+        # total potential q/(4 pi eps_src r) + S[sigma] (test/solver/dielectric_box3d.jl:285-294)
+        r = np.linalg.norm(T[:, None, :] - pos[None, :, :], axis=-1)
+        phi_inc = qs[None, :] / (4 * math.pi * wl["eps_in"] * r)
+        tot_ref, tot = phi_inc + phi_ref, phi_inc + phi_ref2
+        accuracy["probe_potential_rel_err_max"] = float(
+            max(np.linalg.norm(tot[:, c] - tot_ref[:, c]) / np.linalg.norm(tot_ref[:, c]) for c in range(k)))
+        srcs = [bie.PointSource(tuple(p), float(qq)) for p, qq in zip(pos, qs)]
+        W_ref = bie.polarization_energy(itf, np.asfortranarray(S_ref), srcs)
+        W = bie.polarization_energy(itf, np.asfortranarray(S_ref_refined), srcs)
+        accuracy["energy_rel_err_max"] = float(np.max(np.abs(W - W_ref) / np.abs(W_ref)))
+
+    # ---------------- timed: refined (profiled) and plain FP64 ----------------------
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(device) as clk:
+        ms_ref = timed_loop(args.precision, wl["rtol"], profile=True)
+    kt = {}
+    for name, kind in _abi.KERNEL_KINDS.items():
+        t = _abi.KernelTime()
+        _abi.check(L.bie_profile_read(g, kind, C.byref(t)))
+        kt[name] = t
+    _abi.check(L.bie_profile_enable(g, 0))
+    ms_plain = timed_loop("fp64", wl["rtol"])
+
+    total_ms = float(np.sum(ms_ref))
+    total_plain = float(np.sum(ms_plain))
+    if dist is not None:
+        tt = torch.tensor([total_ms, total_plain], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms, total_plain = float(tt[0]), float(tt[1])
+    solves = k * args.steps * world
+    value = solves / (total_ms * 1e-3)
+    plain_value = solves / (total_plain * 1e-3)
+
+    # ---------------- e2e: reference-shaped host API with host buffers ---------------
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    Fh = np.asfortranarray(pin((k, n)).T)   # N x k column-major, pinned
+    Sh = np.asfortranarray(pin((k, n)).T)
+    src_h, q_h, eps_h = pin((k, 3)), pin((k,)), pin((k,))
+    e2e_ms = []
+    o = opts(args.precision, wl["rtol"])
+    for i in range(nsteps):
+        pos_i, q_i = batches[i]
+        src_h[:], q_h[:], eps_h[:] = pos_i, q_i, wl["eps_in"]
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        _abi.check(L.bie_rhs_point(g, _abi.dptr(src_h), _abi.dptr(q_h), _abi.dptr(eps_h), k, _abi.dptr(Fh)))
+        rc = L.bie_solve(g, _abi.dptr(Fh), _abi.dptr(Sh), k, C.byref(o), None)
+        if rc != _abi.BIE_OK:
+            _abi.check(rc)
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_total = float(np.sum(e2e_ms))
+    if dist is not None:
+        tt = torch.tensor([e2e_total], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt[0])
+    e2e_value = solves / (e2e_total * 1e-3)
+
+    # ---------------- roofline of the dominant kernel ------------------------------
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        with open(pk_path) as f:
+            peaks = json.load(f)
+    bf16_peak = peaks.get("bf16_tflops_sustained", 1400.0)
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "of measured" if peaks else "of fallback"
+    clocks = clk.summary()
+    kinds_ms = {nm: t.ms for nm, t in kt.items() if nm != "all"}
+    dominant = max(kinds_ms, key=kinds_ms.get)
+    tc = kt["direct_tc"]
+    roofline = None
+    if tc.launches:
+        per_launch_ms = tc.ms / (tc.launches / 2)  # pack + tensor-core kernel per column block
+        flops = 6.0 * tc.pair_cols / (tc.launches / 2)  # three bf16 MMAs (2 flops each) per pair and column
+        achieved = flops / (per_launch_ms * 1e-3) / 1e12
+        roofline = {"kernel": "k_dt_tc (tcgen05 split-BF16 x3 block direct sum, incl. Q packing)", "bound": "tensor",
+                    "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
+                    "peak_source": f"bf16_tflops_sustained {peak_src}", "traffic": None,
+                    "per_launch_ms": per_launch_ms}
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        fp32_issue_peak = 148 * 128 * sm_mhz * 1e6  # FP32 lane-instructions/s at the sampled clock
+        pairs_per_s = tc.pairs / (tc.launches / 2) / (per_launch_ms * 1e-3)
+        roofline["fp32_issue_frac"] = pairs_per_s * 12 / fp32_issue_peak
+        roofline["pairs_per_s"] = pairs_per_s
+    comb = kt["combine"]
+    extra = {}
+    for nm, t in kt.items():
+        if nm == "all" or not t.launches:
+            continue
+        extra[nm] = {"ms": t.ms, "launches": t.launches, "share": t.ms / max(kt["all"].ms, 1e-9)}
+    if comb.launches:
+        gbs = comb.bytes / (comb.ms * 1e-3) / 1e9
+        extra["combine"].update({"achieved_GBps": gbs, "hbm_frac": gbs / hbm_peak})
+    f64 = kt["direct_fp64"]
+    if f64.launches:
+        extra["direct_fp64"]["pair_cols_per_s"] = f64.pair_cols / (f64.ms * 1e-3)
+
+    # ---------------- CPU baseline (rank 0, N = 1) ----------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        info = cpu_reference(wl, max_seconds=20.0, threads=os.cpu_count())
+        cpu = {"value": 1.0 / info["seconds"], "unit": "solves/s", "cores": info["cores"], "kind": "port",
+               "sample": f"one RHS column of the workload: oracle FP64 direct sum + CSC corrections + GMRES, "
+                         f"{info['iterations']} iterations, {info['seconds']:.2f} s"
+                         f"{'' if info['converged'] else ' (time-bounded, not converged)'}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": f"{args.precision} tensor-core direct sum + fp64",
+            "data": "synthetic (seeded point sources, uniform in the box interior)",
+            "config": workload_config(args.workload, wl, n),
+            "p50_ms": float(np.percentile(ms_ref, 50)), "p99_ms": float(np.percentile(ms_ref, 99)),
+            "plain_fp64": {"value": plain_value, "unit": "solves/s", "ms_per_step": total_plain / args.steps,
+                           "p50_ms": float(np.percentile(ms_plain, 50)),
+                           "p99_ms": float(np.percentile(ms_plain, 99)), "iterations": plain_ref_iters},
+            "speedup_vs_plain_fp64": value / plain_value,
+            "accuracy": accuracy,
+            "roofline": roofline,
+            "kernels": extra,
+            "dominant_kernel_kind": dominant,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": n * k * 8 + 5 * k * 8,
+                    "d2h_bytes_per_step": 2 * n * k * 8},
+            "gpu_launches": int(kt["all"].launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

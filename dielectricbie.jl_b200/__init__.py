@@ -520,7 +520,7 @@ class SolveStats:
 
 
 def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float = 0.0, itmax: int = 500,
-              restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-5, max_outer: int = 8,
+              restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
               precondition: bool = False, check_every: int = 1, raise_on_noconv: bool = False):
     """Solve A Sigma = F on the device. Returns (Sigma, SolveStats)."""
     Ff, vec = _as_cols(F, op.n)

@@ -26,7 +26,7 @@ EXPORTS = [
     "bie_near_destroy", "bie_geom_create", "bie_geom_create_from_mesh", "bie_geom_info", "bie_geom_stream",
     "bie_geom_destroy", "bie_matvec", "bie_matvec_device", "bie_rhs_point", "bie_rhs_point_device",
     "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve",
-    "bie_solve_device",
+    "bie_solve_device", "bie_profile_enable", "bie_profile_read",
 ]
 
 
@@ -50,6 +50,14 @@ class SolveOpts(C.Structure):
     _fields_ = [("atol", C.c_double), ("rtol", C.c_double), ("itmax", C.c_int), ("restart", C.c_int),
                 ("precision", C.c_int), ("inner_rtol", C.c_double), ("max_outer", C.c_int),
                 ("precondition", C.c_int), ("check_every", C.c_int), ("flags", C.c_uint32)]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [("ms", C.c_double), ("launches", C.c_int64), ("pairs", C.c_double), ("pair_cols", C.c_double),
+                ("bytes", C.c_double)]
+
+
+KERNEL_KINDS = {"direct_fp64": 0, "direct_fp32": 1, "direct_tc": 2, "combine": 3, "krylov": 4, "other": 5, "all": 6}
 
 
 class Stats(C.Structure):
@@ -107,6 +115,8 @@ def lib():
         "bie_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
         "bie_solve": (i, [_vp, _dp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats)]),
         "bie_solve_device": (i, [_vp, _vp, _vp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats), _vp]),
+        "bie_profile_enable": (i, [_vp, i]),
+        "bie_profile_read": (i, [_vp, i, C.POINTER(KernelTime)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -358,7 +358,7 @@ void bie_solve_opts_default(bie_solve_opts* o) {
     o->itmax = 500;
     o->restart = 200;
     o->precision = BIE_FP64;
-    o->inner_rtol = 1e-5;
+    o->inner_rtol = 1e-6;
     o->max_outer = 8;
     o->precondition = 0;
     o->check_every = 1;
@@ -386,6 +386,21 @@ int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, c
         rc = bie::solve_device(g, dF, dSigma, k, o ? *o : d, st, (cudaStream_t)stream);
     });
     return grc != BIE_OK ? grc : rc;
+}
+
+// ----------------------------- kernel timing -------------------------------
+int bie_profile_enable(bie_geom* g, int enable) {
+    return guarded([&] {
+        REQUIRE(g, "null geom");
+        bie::profile_enable(g, enable);
+    });
+}
+
+int bie_profile_read(bie_geom* g, int kind, bie_kernel_time* out) {
+    return guarded([&] {
+        REQUIRE(g && out && kind >= 0 && kind <= BIE_KERNEL_KINDS, "profile_read: bad argument");
+        bie::profile_read(g, kind, out);
+    });
 }
 
 }  // extern "C"

@@ -26,9 +26,24 @@ struct bie_geom {
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // kernel timing
+    struct ProfRec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    bool prof_on = false;
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
+    bie_kernel_time acc[BIE_KERNEL_KINDS] = {};
 };
 
 namespace bie {
+
+// Relative errors of the reduced-precision operators (measured on the config boxes:
+// ~4e-6 for the split-BF16 three-term contraction, ~1e-7 for the FP32 direct sum),
+// used to decide when a residual update may run in reduced precision.
+constexpr double kDeltaBF16X3 = 8e-6;
+constexpr double kDeltaFP32 = 3e-7;
 
 namespace {
 
@@ -46,6 +61,64 @@ struct DeviceGuard {
 };
 
 inline unsigned grid1(int64_t n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+cudaEvent_t pool_event(bie_geom* g) {
+    if (!g->ev_pool.empty()) {
+        cudaEvent_t e = g->ev_pool.back();
+        g->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    BIE_CK(cudaEventCreate(&e));
+    return e;
+}
+
+void prof_drain(bie_geom* g) {
+    for (auto& r : g->prof_pending) {
+        BIE_CK(cudaEventSynchronize(r.b));
+        float ms = 0.f;
+        BIE_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        g->acc[r.kind].ms += ms;
+        g->ev_pool.push_back(r.a);
+        g->ev_pool.push_back(r.b);
+    }
+    g->prof_pending.clear();
+}
+
+// Scope around the launches of one kernel kind: counts launches and algorithmic
+// units always, and brackets them with CUDA events on `s` while timing is enabled.
+struct Prof {
+    bie_geom* g;
+    int kind;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr;
+    Prof(bie_geom* g_, int kind_, cudaStream_t s_, int launches = 1, double pairs = 0, double pair_cols = 0,
+         double bytes = 0)
+        : g(g_), kind(kind_), s(s_) {
+        bie_kernel_time& t = g->acc[kind];
+        t.launches += launches;
+        t.pairs += pairs;
+        t.pair_cols += pair_cols;
+        t.bytes += bytes;
+        if (g->prof_on) {
+            if (g->prof_pending.size() > 8192) prof_drain(g);
+            a = pool_event(g);
+            BIE_CK(cudaEventRecord(a, s));
+        }
+    }
+    ~Prof() {
+        if (!a) return;
+        cudaEvent_t b = nullptr;
+        if (!g->ev_pool.empty()) {
+            b = g->ev_pool.back();
+            g->ev_pool.pop_back();
+        } else if (cudaEventCreate(&b) != cudaSuccess) {
+            return;
+        }
+        cudaEventRecord(b, s);
+        g->prof_pending.push_back({kind, a, b});
+    }
+};
 
 GeomDev gdev(const bie_geom* g) {
     return GeomDev{g->x.as<double>(), g->y.as<double>(), g->z.as<double>(), g->nx.as<double>(),
@@ -150,8 +223,12 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
     Split sp = choose_split(rows, g->n, g->sms, occ_for(kind, Cmax));
     g->part.ensure(sizeof(double) * (size_t)sp.nsplit * std::max<int64_t>(rows, 1) * k);
     double* part = g->part.as<double>();
+    const int pkind = kind == Kern::DT64 ? BIE_KERNEL_DIRECT_FP64
+                      : (kind == Kern::DT32 ? BIE_KERNEL_DIRECT_FP32 : BIE_KERNEL_OTHER);
+    const double npairs = kind == Kern::POT64 ? (double)M * g->n : (double)g->n * (g->n - 1);
     for (int c0 = 0; c0 < k;) {
         int C = pick_C(k - c0);
+        Prof pf(g, pkind, s, 1, npairs, npairs * C);
         switch (C) {
             case 64: launch_direct<64>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
             case 32: launch_direct<32>(kind, gd, X, ldx, c0, pre, T, M, sp, part, k, s); break;
@@ -187,6 +264,8 @@ Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, cuda
     g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 256)));
     for (int c0 = 0; c0 < k; c0 += 256) {
         int kc = std::min(256, k - c0);
+        const double npairs = (double)g->n * (g->n - 1);
+        Prof pf(g, BIE_KERNEL_DIRECT_TC, s, 2, npairs, npairs * tc_npad(kc));
         launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, g->bpack.as<uint8_t>(),
                         g->errflag.as<int>(), s);
     }
@@ -205,6 +284,10 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
     }
     const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
     const bool dg = !(flags & BIE_NO_DIAG);
+    const double cbytes = (corr ? (double)g->nblocks * g->nb * g->nb * 8 + g->nblocks * 4.0 + (g->npanels + 1) * 4.0
+                                : 0.0) +
+                          (double)g->n * k * 8 * (2 + sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
+    Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
     k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
                                               dg ? g->diag.as<double>() : nullptr,
                                               corr ? g->rowptr.as<int32_t>() : nullptr,
@@ -239,6 +322,7 @@ void dots(bie_geom* g, const double* A, int64_t strideA, int nv, const double* B
     DotPlan p = dot_plan(g->n, k, nv);
     g->dpart.ensure(sizeof(double) * (size_t)p.nblk * nv * k);
     dim3 grid(p.nblk, nv);
+    Prof pf(g, BIE_KERNEL_KRYLOV, s, 2);
     k_dots_partial<<<grid, p.bs, p.bs * sizeof(double), s>>>(A, strideA, nv, B, g->n, k, p.rows_per_blk,
                                                             g->dpart.as<double>(), p.nblk);
     BIE_CK(cudaGetLastError());
@@ -308,7 +392,10 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             apply_op(g, dx, W, k, prec, flags, pre, s);
             ++res.matvecs;
             BIE_CK(cudaMemcpyAsync(g->rr.p, dr, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
-            k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, W, 1.0, g->rr.as<double>(), n, k, nullptr);
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, W, 1.0, g->rr.as<double>(), n, k, nullptr);
+            }
             r = g->rr.as<double>();
         }
         col_norms(g, r, k, g->beta.as<double>(), s);
@@ -327,7 +414,10 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
         BIE_CK(cudaMemsetAsync(g->jlast.p, 0, sizeof(int) * k, s));
         BIE_CK(cudaMemsetAsync(g->gv.p, 0, sizeof(double) * m1 * k, s));
         BIE_CK(cudaMemcpyAsync(g->gv.p, g->beta.p, sizeof(double) * k, cudaMemcpyDeviceToDevice, s));
-        k_scale_cols<<<grid1(nk), 256, 0, s>>>(r, g->beta.as<double>(), n, k, V);
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            k_scale_cols<<<grid1(nk), 256, 0, s>>>(r, g->beta.as<double>(), n, k, V);
+        }
         int j = 0;
         bool any = true;
         for (; j < m && it < itmax; ++j) {
@@ -336,17 +426,32 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             ++res.matvecs;
             // classical Gram-Schmidt, twice
             dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
-            k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+            }
             dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
-            k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h2.as<double>(), n, k);
-            k_axpby<<<grid1((j + 1) * k), 256, 0, s>>>(1.0, g->h2.as<double>(), 1.0, g->h.as<double>(), j + 1, k,
-                                                        nullptr);
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h2.as<double>(), n, k);
+            }
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_axpby<<<grid1((j + 1) * k), 256, 0, s>>>(1.0, g->h2.as<double>(), 1.0, g->h.as<double>(), j + 1, k,
+                nullptr);
+            }
             col_norms(g, W, k, g->hn.as<double>(), s);
-            k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
-            k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->hn.as<double>(),
-                                                 g->cs.as<double>(), g->sn.as<double>(), g->gv.as<double>(),
-                                                 g->active.as<int>(), g->jlast.as<int>(), g->eps.as<double>(),
-                                                 g->resid.as<double>(), j, m1, k);
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
+            }
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->hn.as<double>(),
+                g->cs.as<double>(), g->sn.as<double>(), g->gv.as<double>(),
+                g->active.as<int>(), g->jlast.as<int>(), g->eps.as<double>(),
+                g->resid.as<double>(), j, m1, k);
+            }
             BIE_CK(cudaGetLastError());
             ++it;
             if ((j + 1) % std::max(1, check_every) == 0 || j + 1 == m || it >= itmax) {
@@ -359,9 +464,15 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
                 }
             }
         }
-        k_backsolve<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->gv.as<double>(), g->jlast.as<int>(), m1, k,
-                                                 g->yv.as<double>());
-        k_update_solution<<<grid1(nk), 256, 0, s>>>(dx, V, nk, g->yv.as<double>(), g->jlast.as<int>(), m, pre, n, k);
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            k_backsolve<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->gv.as<double>(), g->jlast.as<int>(), m1, k,
+            g->yv.as<double>());
+        }
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            k_update_solution<<<grid1(nk), 256, 0, s>>>(dx, V, nk, g->yv.as<double>(), g->jlast.as<int>(), m, pre, n, k);
+        }
         BIE_CK(cudaGetLastError());
         d2h(jl.data(), g->jlast.p, k, s);
         for (int c = 0; c < k; ++c) res.col_iters[c] += jl[c];
@@ -458,6 +569,11 @@ void geom_destroy(bie_geom* g) {
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
                            &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
         for (auto* b : all) b->release();
+        for (auto& r : g->prof_pending) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        for (auto e : g->ev_pool) cudaEventDestroy(e);
         if (g->ev0) cudaEventDestroy(g->ev0);
         if (g->ev1) cudaEventDestroy(g->ev1);
         if (g->stream) cudaStreamDestroy(g->stream);
@@ -472,6 +588,28 @@ void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes) {
 }
 
 void* geom_stream(bie_geom* g) { return (void*)g->stream; }
+
+void profile_enable(bie_geom* g, int on) {
+    DeviceGuard dg(g->device);
+    prof_drain(g);
+    if (on)
+        for (auto& t : g->acc) t = bie_kernel_time{};
+    g->prof_on = on != 0;
+}
+
+void profile_read(bie_geom* g, int kind, bie_kernel_time* out) {
+    DeviceGuard dg(g->device);
+    prof_drain(g);
+    if (kind == BIE_KERNEL_KINDS) {
+        bie_kernel_time t{};
+        for (auto& a : g->acc) {
+            t.ms += a.ms; t.launches += a.launches; t.pairs += a.pairs; t.pair_cols += a.pair_cols; t.bytes += a.bytes;
+        }
+        *out = t;
+    } else {
+        *out = g->acc[kind];
+    }
+}
 
 // ---------------------------------------------------------------------------
 // operators
@@ -492,9 +630,15 @@ void matvec_host(bie_geom* g, const double* X, double* Y, int k, int precision, 
     g->io_b.ensure(sizeof(double) * nk);
     g->xo.ensure(sizeof(double) * nk);
     BIE_CK(cudaMemcpyAsync(g->io_a.p, X, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
-    k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    }
     apply_op(g, g->io_b.as<double>(), g->xo.as<double>(), k, precision, flags, nullptr, s);
-    k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->xo.as<double>(), g->n, k, g->io_a.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->xo.as<double>(), g->n, k, g->io_a.as<double>());
+    }
     BIE_CK(cudaGetLastError());
     BIE_CK(cudaMemcpyAsync(Y, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));
@@ -505,7 +649,10 @@ void rhs_point_device(bie_geom* g, const double* src, const double* q, const dou
                       cudaStream_t s) {
     DeviceGuard dg(g->device);
     if (!s) s = g->stream;
-    k_rhs_point<<<grid1(g->n * k), 256, 0, s>>>(gdev(g), src, q, eps, k, F);
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_rhs_point<<<grid1(g->n * k), 256, 0, s>>>(gdev(g), src, q, eps, k, F);
+    }
     BIE_CK(cudaGetLastError());
 }
 
@@ -521,8 +668,14 @@ void rhs_point_host(bie_geom* g, const double* src, const double* q, const doubl
     g->io_a.ensure(sizeof(double) * nk);
     g->io_b.ensure(sizeof(double) * nk);
     const double* d = g->small.as<double>();
-    k_rhs_point<<<grid1(nk), 256, 0, s>>>(gdev(g), d, d + 3 * k, d + 4 * k, k, g->io_b.as<double>());
-    k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->io_b.as<double>(), g->n, k, g->io_a.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_rhs_point<<<grid1(nk), 256, 0, s>>>(gdev(g), d, d + 3 * k, d + 4 * k, k, g->io_b.as<double>());
+    }
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->io_b.as<double>(), g->n, k, g->io_a.as<double>());
+    }
     BIE_CK(cudaGetLastError());
     BIE_CK(cudaMemcpyAsync(F, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));
@@ -533,7 +686,10 @@ void potential_device(bie_geom* g, const double* S, int k, const double* T, int6
     if (!s) s = g->stream;
     if (M == 0) return;
     Split sp = direct_sum(g, Kern::POT64, S, k, k, nullptr, T, M, s);
-    k_reduce_parts<<<grid1(M * k), 256, 0, s>>>(g->part.as<double>(), sp.nsplit, M, k, kInv4Pi, phi);
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_reduce_parts<<<grid1(M * k), 256, 0, s>>>(g->part.as<double>(), sp.nsplit, M, k, kInv4Pi, phi);
+    }
     BIE_CK(cudaGetLastError());
 }
 
@@ -547,9 +703,15 @@ void potential_host(bie_geom* g, const double* S, int k, const double* T, int64_
     g->xo.ensure(sizeof(double) * M * k);
     upload(g->small, T, (size_t)3 * M, s);
     BIE_CK(cudaMemcpyAsync(g->io_a.p, S, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
-    k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    }
     potential_device(g, g->io_b.as<double>(), k, g->small.as<double>(), M, g->xo.as<double>(), s);
-    k_nodemajor_to_colmajor<<<grid1(M * k), 256, 0, s>>>(g->xo.as<double>(), M, k, g->io_a.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_nodemajor_to_colmajor<<<grid1(M * k), 256, 0, s>>>(g->xo.as<double>(), M, k, g->io_a.as<double>());
+    }
     BIE_CK(cudaGetLastError());
     BIE_CK(cudaMemcpyAsync(phi, g->io_a.p, sizeof(double) * M * k, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));
@@ -599,24 +761,24 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
         col_it = r.col_iters;
     } else {
         BIE_CK(cudaMemsetAsync(dX, 0, sizeof(double) * nk, s));
+        // FP64 iterative refinement. The residual r = F - A x is kept in FP64. After a
+        // correction d it is refreshed either with the full FP64 operator
+        // (r = F - A64 x) or, once the residual is small, updated with the
+        // reduced-precision operator (r -= A_low d): that update errs by about
+        // delta * ||A d|| ~ delta * ||r||, delta being the operator's relative error,
+        // which is admitted only while it stays below a quarter of the tolerance.
+        const double delta = o.precision == BIE_BF16X3 ? kDeltaBF16X3 : kDeltaFP32;
         std::vector<double> rn = fn, eps_in(k);
-        const double* rhs = dF;
+        BIE_CK(cudaMemcpyAsync(rbuf, dF, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
+        have_true_resid = true;
         for (int it_out = 0;; ++it_out) {
-            if (it_out > 0) {
-                // FP64 outer residual r = F - A x
-                apply_op(g, dX, rbuf, k, BIE_FP64, o.flags, nullptr, s);
-                ++f64mv;
-                k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, dF, -1.0, rbuf, n, k, nullptr);
-                col_norms(g, rbuf, k, g->small.as<double>(), s);
-                d2h(rn.data(), g->small.p, k, s);
-                rhs = rbuf;
-                have_true_resid = true;
-            }
             int nact = 0;
+            bool lowp_update_ok = true;
             for (int c = 0; c < k; ++c) {
                 act[c] = rn[c] > tol[c] ? 1 : 0;
                 nact += act[c];
                 rel[c] = fn[c] > 0 ? rn[c] / fn[c] : 0.0;
+                if (act[c] && delta * rn[c] > 0.25 * tol[c]) lowp_update_ok = false;
             }
             if (nact == 0) {
                 converged = true;
@@ -624,22 +786,45 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             }
             if (it_out >= o.max_outer || iters >= o.itmax) break;
             for (int c = 0; c < k; ++c) eps_in[c] = std::max(o.inner_rtol * rn[c], 0.5 * tol[c]);
-            GmresResult r = gmres(g, rhs, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
+            GmresResult r = gmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
                                   o.itmax - iters, o.restart, o.check_every, s);
             iters += r.iters;
             lpmv += r.matvecs;
             for (int c = 0; c < k; ++c) col_it[c] += r.col_iters[c];
             upload(g->active, std::vector<int>(act.begin(), act.end()).data(), k, s);
-            k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, g->dd.as<double>(), 1.0, dX, n, k, g->active.as<int>());
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, g->dd.as<double>(), 1.0, dX, n, k, g->active.as<int>());
+            }
             BIE_CK(cudaGetLastError());
             ++outer;
+            if (lowp_update_ok) {
+                // r -= A_low d  (d = 0 in the frozen columns)
+                apply_op(g, g->dd.as<double>(), g->rr.as<double>(), k, o.precision, o.flags, nullptr, s);
+                ++lpmv;
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, g->rr.as<double>(), 1.0, rbuf, n, k, nullptr);
+                have_true_resid = false;
+            } else {
+                // r = F - A64 x
+                apply_op(g, dX, rbuf, k, BIE_FP64, o.flags, nullptr, s);
+                ++f64mv;
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, dF, -1.0, rbuf, n, k, nullptr);
+                have_true_resid = true;
+            }
+            col_norms(g, rbuf, k, g->small.as<double>(), s);
+            d2h(rn.data(), g->small.p, k, s);
         }
     }
     const bool verify = !(o.flags & 4u) && (st != nullptr);
     if (verify && !have_true_resid) {
         apply_op(g, dX, rbuf, k, BIE_FP64, o.flags, nullptr, s);
         ++f64mv;
-        k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, dF, -1.0, rbuf, n, k, nullptr);
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, dF, -1.0, rbuf, n, k, nullptr);
+        }
         std::vector<double> rn(k);
         col_norms(g, rbuf, k, g->small.as<double>(), s);
         d2h(rn.data(), g->small.p, k, s);
@@ -681,9 +866,15 @@ int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_sol
     g->io_b.ensure(sizeof(double) * nk);
     g->sol.ensure(sizeof(double) * nk);  // output buffer, never aliased by the solver's scratch
     BIE_CK(cudaMemcpyAsync(g->io_a.p, F, sizeof(double) * nk, cudaMemcpyHostToDevice, s));
-    k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_colmajor_to_nodemajor<<<grid1(nk), 256, 0, s>>>(g->io_a.as<double>(), g->n, k, g->io_b.as<double>());
+    }
     int rc = solve_device(g, g->io_b.as<double>(), g->sol.as<double>(), k, o, st, s);
-    k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->sol.as<double>(), g->n, k, g->io_a.as<double>());
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->sol.as<double>(), g->n, k, g->io_a.as<double>());
+    }
     BIE_CK(cudaGetLastError());
     BIE_CK(cudaMemcpyAsync(Sigma, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));

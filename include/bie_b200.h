@@ -51,6 +51,8 @@ typedef enum {
 /* matvec flags */
 #define BIE_NO_CORRECTIONS 1u /* skip the near-field correction blocks */
 #define BIE_NO_DIAG 2u        /* skip the diagonal contrast term */
+#define BIE_NO_VERIFY 4u      /* solve: skip the final FP64 true-residual evaluation (stats then
+                                 report the solver's own residual estimate) */
 
 /* Copies the message of the last failed call on this thread (always NUL-terminated).
  * Returns the full message length. */
@@ -172,7 +174,7 @@ typedef struct {
     int itmax;           /* maximum Krylov iterations in total (default 500) */
     int restart;         /* Krylov basis capacity before restart (default 200) */
     int precision;       /* bie_precision of the Krylov operator (default BIE_FP64) */
-    double inner_rtol;   /* mixed precision: relative tolerance of each inner solve (default 1e-5) */
+    double inner_rtol;   /* mixed precision: relative tolerance of each inner solve (default 1e-6) */
     int max_outer;       /* mixed precision: maximum refinement steps (default 8) */
     int precondition;    /* right diagonal preconditioner 1/t_P (src/solver/multi_rhs.jl:234-247) */
     int check_every;     /* host convergence check period in iterations (default 1) */
@@ -186,7 +188,8 @@ typedef struct {
     int fp64_matvecs;     /* full FP64 operator applications */
     int lowp_matvecs;     /* reduced-precision operator applications */
     int converged;        /* all columns reached atol + rtol * ||F[:, c]|| */
-    double max_rel_resid; /* max_c ||F - A Sigma||_c / ||F||_c, FP64 true residual */
+    double max_rel_resid; /* max_c ||F - A Sigma||_c / ||F||_c: the FP64 true residual unless
+                             BIE_NO_VERIFY is set, else the maintained residual */
     double seconds;       /* device time of the solve */
     int* col_iterations;  /* optional (k entries): Krylov iterations per column */
     double* col_resid;    /* optional (k entries): final true relative residual per column */
@@ -202,6 +205,32 @@ typedef struct {
 int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st);
 int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o,
                      bie_stats* st, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Kernel timing (CUDA events on the launching stream)                        */
+/* ------------------------------------------------------------------------- */
+typedef enum {
+    BIE_KERNEL_DIRECT_FP64 = 0,  /* K1 FP64 direct sum */
+    BIE_KERNEL_DIRECT_FP32 = 1,  /* K2 FP32 direct sum */
+    BIE_KERNEL_DIRECT_TC = 2,    /* K3 tensor-core block direct sum (incl. its Q packing) */
+    BIE_KERNEL_COMBINE = 3,      /* K4+K5 partial reduction + BSR corrections + diagonal */
+    BIE_KERNEL_KRYLOV = 4,       /* K7 orthogonalisation, Givens, updates */
+    BIE_KERNEL_OTHER = 5,        /* right-hand sides, potentials, layout conversions */
+    BIE_KERNEL_KINDS = 6
+} bie_kernel_kind;
+
+typedef struct {
+    double ms;          /* summed device time of the launches */
+    int64_t launches;   /* kernel launches */
+    double pairs;       /* target-source pair interactions (direct sums) */
+    double pair_cols;   /* pairs x right-hand-side columns (direct sums; padded columns for K3) */
+    double bytes;       /* algorithmic bytes (combine: BSR values/indices + vectors) */
+} bie_kernel_time;
+
+/* Starts (enable = 1, counters reset) or stops (0) event timing of the handle's launches. */
+int bie_profile_enable(bie_geom* g, int enable);
+/* Reads the accumulated figures of one kernel kind (synchronises the stream). */
+int bie_profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 
 #ifdef __cplusplus
 }
