@@ -13,10 +13,13 @@
 // G Q ~= Gh Qh + Gh Ql + Gl Qh (the dropped Gl Ql term is ~2^-16 relative),
 // accumulated in FP32 in tensor memory; each source split writes an FP64 partial.
 //
-// CTA = 192 threads: warps 0-3 generate the 128 x 64 kernel tile of a source
-// chunk (one thread per target row, K-major rows in the 128-byte swizzled
-// layout the UMMA descriptors read) and run the epilogue; warp 4 issues the
-// MMAs (one thread); warp 5 streams the pre-swizzled Q tiles with bulk copies.
+// CTA = 320 threads: warps 0-7 generate the 128 x 64 kernel tile of a source
+// chunk (two threads per target row, each writing 32 of the row's 64 K-major
+// bf16 values into the 128-byte swizzled layout the UMMA descriptors read) and
+// run the epilogue; warp 8 issues the MMAs (one thread); warp 9 streams the
+// pre-swizzled Q tiles with bulk copies. Box faces are axis-aligned, so a warp
+// whose 32 rows share a normal axis computes n.(x - y) as the signed axis
+// difference and folds the sign into its epilogue.
 // Every mbarrier wait is bounded: on expiry the CTA records an error code and
 // returns after releasing its tensor memory.
 #include <cuda_bf16.h>
@@ -33,7 +36,8 @@ namespace tc {
 constexpr int M = 128;      // targets per tile (MMA M)
 constexpr int KC = 64;      // sources per chunk = one 128-byte bf16 row
 constexpr int S = 2;        // pipeline stages
-constexpr int NTHREADS = 192;
+constexpr int NGEN = 256;      // generator threads: 2 per tile row (two halves of a chunk)
+constexpr int NTHREADS = NGEN + 64;
 constexpr uint32_t kWaitLimit = 1u << 26;
 constexpr int kErrTimeout = 1;
 
@@ -88,14 +92,14 @@ __device__ __forceinline__ bool mbar_wait_raw(uint64_t* b, uint32_t parity) {
     return false;
 }
 
-// OR-reduction of a predicate over the 128 generator threads (named barrier 1):
+// OR-reduction of a predicate over the 256 generator threads (named barrier 1):
 // also orders their shared-memory accesses like bar.sync.
 __device__ __forceinline__ bool gen_any(bool v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, 1, 128, q;\n\t"
+        "bar.red.or.pred p, 1, 256, q;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(r)
         : "r"((uint32_t)v)
@@ -153,6 +157,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
+// MUFU reciprocal square root (approximate, flush-to-zero): one instruction.
+__device__ __forceinline__ float rsqrt_mufu(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
     __nv_bfloat162 h = __floats2bfloat162_rn(lo_elem, hi_elem);  // .x (low 16 bits) = lo_elem
     return *reinterpret_cast<uint32_t*>(&h);
@@ -163,6 +174,45 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
     hi = pack_bf16(a, b);
     float ah = __uint_as_float(hi << 16), bh = __uint_as_float(hi & 0xFFFF0000u);
     lo = pack_bf16(a - ah, b - bh);
+}
+
+// One thread's half row of a chunk's kernel tile: 32 sources (groups gq0..gq0+3).
+// AX = 0/1/2: the rows of this warp have normal +-e_AX (sign applied in the
+// epilogue); AX = 3: general normal.
+template <int AX>
+__device__ __forceinline__ void gen_half_row(const float4* __restrict__ cs, float xi, float yi, float zi, float n0,
+                                             float n1, float n2, int gq0, bool self, int64_t j0, int64_t i,
+                                             uint8_t* Ah, uint8_t* Al, uint32_t row_off, uint32_t rsw) {
+#pragma unroll 1
+    for (int gq = gq0; gq < gq0 + 4; ++gq) {
+        float v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const float4 c = cs[gq * 8 + e];
+            const float dx = xi - c.x, dy = yi - c.y, dz = zi - c.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float ri = rsqrt_mufu(r2);
+            float dn;
+            if (AX == 0) dn = dx;
+            else if (AX == 1) dn = dy;
+            else if (AX == 2) dn = dz;
+            else dn = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+            v[e] = (dn * ri) * (ri * ri);
+        }
+        if (self) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if (j0 + gq * 8 + e == i) v[e] = 0.f;
+        }
+        uint4 h, l;
+        split2(v[0], v[1], h.x, l.x);
+        split2(v[2], v[3], h.y, l.y);
+        split2(v[4], v[5], h.z, l.z);
+        split2(v[6], v[7], h.w, l.w);
+        const uint32_t off = row_off + ((((uint32_t)gq) ^ rsw) << 4);
+        *reinterpret_cast<uint4*>(Ah + off) = h;
+        *reinterpret_cast<uint4*>(Al + off) = l;
+    }
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
@@ -192,7 +242,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
-            mbar_init(&full_a[s], 128);
+            mbar_init(&full_a[s], NGEN);
             mbar_init(&full_b[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -215,9 +265,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     const int64_t io = min(i0, n - 1);
     const double ox = P.g.x[io], oy = P.g.y[io], oz = P.g.z[io];
 
-    if (warp < 4) {
+    if (warp < NGEN / 32) {
         // ------------------------- generators -------------------------------
-        const int r = threadIdx.x;  // tile row
+        const int r = threadIdx.x & (M - 1);  // tile row
+        const int half = threadIdx.x / M;     // which 32 sources of each chunk
         const int64_t i = i0 + r;
         const bool valid = i < n;
         float xi, yi, zi, n0, n1, n2;
@@ -228,6 +279,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             xi = yi = zi = -1.0e18f;  // far from every node and every padded source: G underflows to 0
             n0 = n1 = n2 = 0.f;
         }
+        // warp-uniform normal axis (code 0/1/2 = +-e_axis, 3 = general)
+        int code = 3;
+        float sgn = 1.f;
+        if (fabsf(n0) == 1.f && n1 == 0.f && n2 == 0.f) { code = 0; sgn = n0; }
+        else if (fabsf(n1) == 1.f && n0 == 0.f && n2 == 0.f) { code = 1; sgn = n1; }
+        else if (fabsf(n2) == 1.f && n0 == 0.f && n1 == 0.f) { code = 2; sgn = n2; }
+        const unsigned full = 0xFFFFFFFFu;
+        const int cmin = __reduce_min_sync(full, valid ? code : 4);
+        const int cmax = __reduce_max_sync(full, valid ? code : -1);
+        const int ax = (cmin == cmax && cmin < 3) ? cmin : 3;
+        if (ax == 3) sgn = 1.f;
         const uint32_t row_off = (uint32_t)r * 128u;
         const uint32_t rsw = (uint32_t)(r & 7);
         for (int lc = 0; lc < nch; ++lc) {
@@ -249,31 +311,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             uint8_t* Al = A + (s * 2 + 1) * a_bytes;
             const float4* cs = crd + s * KC;
             const bool self = (j0 < i0 + M) && (j0 + KC > i0);
-#pragma unroll 1
-            for (int gq = 0; gq < KC / 8; ++gq) {
-                float v[8];
-#pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    const float4 c = cs[gq * 8 + e];
-                    float dx = xi - c.x, dy = yi - c.y, dz = zi - c.z;
-                    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    float ri = rsqrtf(r2);
-                    float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
-                    v[e] = nd * (ri * ri * ri);
-                }
-                if (self) {
-#pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        if (j0 + gq * 8 + e == i) v[e] = 0.f;
-                }
-                uint4 h, l;
-                split2(v[0], v[1], h.x, l.x);
-                split2(v[2], v[3], h.y, l.y);
-                split2(v[4], v[5], h.z, l.z);
-                split2(v[6], v[7], h.w, l.w);
-                const uint32_t off = row_off + ((((uint32_t)gq) ^ rsw) << 4);
-                *reinterpret_cast<uint4*>(Ah + off) = h;
-                *reinterpret_cast<uint4*>(Al + off) = l;
+            const int gq0 = half * 4;
+            switch (ax) {
+                case 0: gen_half_row<0>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
+                case 1: gen_half_row<1>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
+                case 2: gen_half_row<2>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
+                default: gen_half_row<3>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&full_a[s]);
@@ -284,9 +327,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
         ok = !gen_any(!ok);  // every generator warp takes the same branch
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (ok) {
-            const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+            const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
             double* out = P.part + ((int64_t)blockIdx.y * n + i) * P.ldp + P.c0;
-            for (int c = 0; c < npad; c += 16) {
+            for (int c = half * 16; c < npad; c += 32) {
                 float v[16];
                 if (nch > 0) {
                     tmem_ld16(tmem + lane_base + (uint32_t)c, v);
@@ -297,11 +340,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
                 if (valid) {
 #pragma unroll
                     for (int q = 0; q < 16; ++q)
-                        if (c + q < P.keff) out[c + q] = (double)v[q];
+                        if (c + q < P.keff) out[c + q] = (double)(sgn * v[q]);
                 }
             }
         }
-    } else if (warp == 4) {
+    } else if (warp == NGEN / 32) {
         // ------------------------- MMA issuer --------------------------------
         if (lane == 0) {
             const uint32_t idesc = idesc_bf16(npad);

@@ -9,6 +9,13 @@ constexpr double kInv4Pi = 0.079577471545947667884;  // 1 / (4 pi)
 constexpr int kTB = 128;  // targets per CTA of the direct-sum kernels (one per thread)
 constexpr int kTS = 128;  // sources per shared-memory tile
 
+// MUFU reciprocal square root (approximate, flush-to-zero): a single instruction.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Device-resident geometry: SoA FP64 arrays of length n.
 struct GeomDev {
     const double *x, *y, *z;     // node positions

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restr
             for (int t = 0; t < cnt; ++t) {
                 float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
                 float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                float ri = rsqrtf(r2);
+                float ri = rsqrt_approx(r2);
                 float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
                 float gk = nd * ri * (ri * ri);
 #pragma unroll
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restr
                 if (jt + t == i) continue;
                 float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
                 float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                float ri = rsqrtf(r2);
+                float ri = rsqrt_approx(r2);
                 float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
                 float gk = nd * ri * (ri * ri);
 #pragma unroll
@@ -263,6 +263,74 @@ __global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int
     }
     if (diag) s += diag[i] * (pre ? pre[i] : 1.0) * X[i * ldx + c];
     Y[i * ldy + c] = s;
+}
+
+// K4 + K5, block-row form: one CTA per target panel P (nb consecutive rows).
+// Each block (P, Q) of the row is staged once in shared memory together with the
+// nb x kt slab of (p X)[Q rows] it multiplies, so block values and source slabs
+// are read once per panel (coalesced, 128-bit where aligned) instead of once per
+// output. Then Y[i][c] = (1/4pi) sum_s part[s][i][c] + sum_b B . X + t_i p_i X[i][c]
+// for the panel's rows, columns processed in tiles of at most kKT.
+constexpr int kKT = 64;         // column tile of the block-row combine
+constexpr int kCombOut = 16;    // outputs per thread (nb * kt <= blockDim * kCombOut)
+__global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const double* __restrict__ part, int nsplit,
+                                                       const double* __restrict__ X, const double* __restrict__ pre,
+                                                       const double* __restrict__ diag,
+                                                       const int32_t* __restrict__ rowptr,
+                                                       const int32_t* __restrict__ col,
+                                                       const double* __restrict__ val, int nb,
+                                                       double* __restrict__ Y) {
+    extern __shared__ double smc[];
+    const int P = blockIdx.x;
+    const int64_t row0 = (int64_t)P * nb;
+    const int nb2 = nb * nb;
+    double* sv = smc;          // [nb][nb], column-major block (sv[q * nb + r])
+    double* sx = smc + nb2;    // [nb][kt]
+    const int64_t tot = n * (int64_t)k;
+    const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
+    for (int c0 = 0; c0 < k; c0 += kKT) {
+        const int kt = min(kKT, k - c0);
+        const int nout = nb * kt;
+        double acc[kCombOut];
+#pragma unroll
+        for (int m = 0; m < kCombOut; ++m) acc[m] = 0.0;
+        for (int b = b0; b < b1; ++b) {
+            __syncthreads();
+            const double* vb = val + (int64_t)b * nb2;
+            for (int e = threadIdx.x; e < nb2; e += blockDim.x) sv[e] = vb[e];
+            const int64_t base = (int64_t)col[b] * nb;
+            for (int e = threadIdx.x; e < nout; e += blockDim.x) {
+                const int q = e / kt, c = e - q * kt;
+                double x = X[(base + q) * k + c0 + c];
+                sx[e] = pre ? pre[base + q] * x : x;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < kCombOut; ++m) {
+                const int o = threadIdx.x + m * blockDim.x;
+                if (o < nout) {
+                    const int r = o / kt, c = o - r * kt;
+                    double a = acc[m];
+                    for (int q = 0; q < nb; ++q) a = fma(sv[q * nb + r], sx[q * kt + c], a);
+                    acc[m] = a;
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < kCombOut; ++m) {
+            const int o = threadIdx.x + m * blockDim.x;
+            if (o < nout) {
+                const int r = o / kt, c = o - r * kt;
+                const int64_t i = row0 + r;
+                const int64_t e = i * k + c0 + c;
+                double s = 0.0;
+                for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
+                s = s * kInv4Pi + acc[m];
+                if (diag) s += diag[i] * (pre ? pre[i] : 1.0) * X[e];
+                Y[e] = s;
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

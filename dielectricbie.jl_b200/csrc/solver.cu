@@ -42,7 +42,7 @@ namespace bie {
 // Relative errors of the reduced-precision operators (measured on the config boxes:
 // ~4e-6 for the split-BF16 three-term contraction, ~1e-7 for the FP32 direct sum),
 // used to decide when a residual update may run in reduced precision.
-constexpr double kDeltaBF16X3 = 8e-6;
+constexpr double kDeltaBF16X3 = 4e-6;
 constexpr double kDeltaFP32 = 3e-7;
 
 namespace {
@@ -288,11 +288,24 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
                                 : 0.0) +
                           (double)g->n * k * 8 * (2 + sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
     Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
-    k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
-                                              dg ? g->diag.as<double>() : nullptr,
-                                              corr ? g->rowptr.as<int32_t>() : nullptr,
-                                              corr ? g->col.as<int32_t>() : nullptr,
-                                              corr ? g->val.as<double>() : nullptr, g->nb, Y, k);
+    if (g->nb > 0 && (int64_t)g->npanels * g->nb == g->n && (int64_t)g->nb * std::min(k, kKT) <= 256 * kCombOut) {
+        const size_t sm = sizeof(double) * ((size_t)g->nb * g->nb + (size_t)g->nb * std::min(k, kKT));
+        static bool attr = false;
+        if (!attr) {
+            BIE_CK(cudaFuncSetAttribute(k_combine_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+            attr = true;
+        }
+        k_combine_panel<<<(unsigned)g->npanels, 256, sm, s>>>(
+            g->n, k, g->part.as<double>(), sp.nsplit, X, pre, dg ? g->diag.as<double>() : nullptr,
+            corr ? g->rowptr.as<int32_t>() : nullptr, corr ? g->col.as<int32_t>() : nullptr,
+            corr ? g->val.as<double>() : nullptr, g->nb, Y);
+    } else {
+        k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
+                                                  dg ? g->diag.as<double>() : nullptr,
+                                                  corr ? g->rowptr.as<int32_t>() : nullptr,
+                                                  corr ? g->col.as<int32_t>() : nullptr,
+                                                  corr ? g->val.as<double>() : nullptr, g->nb, Y, k);
+    }
     BIE_CK(cudaGetLastError());
 }
 
@@ -766,7 +779,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
         // (r = F - A64 x) or, once the residual is small, updated with the
         // reduced-precision operator (r -= A_low d): that update errs by about
         // delta * ||A d|| ~ delta * ||r||, delta being the operator's relative error,
-        // which is admitted only while it stays below a quarter of the tolerance.
+        // which is admitted only while it stays below half the tolerance.
         const double delta = o.precision == BIE_BF16X3 ? kDeltaBF16X3 : kDeltaFP32;
         std::vector<double> rn = fn, eps_in(k);
         BIE_CK(cudaMemcpyAsync(rbuf, dF, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
@@ -778,7 +791,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
                 act[c] = rn[c] > tol[c] ? 1 : 0;
                 nact += act[c];
                 rel[c] = fn[c] > 0 ? rn[c] / fn[c] : 0.0;
-                if (act[c] && delta * rn[c] > 0.25 * tol[c]) lowp_update_ok = false;
+                if (act[c] && delta * rn[c] > 0.5 * tol[c]) lowp_update_ok = false;
             }
             if (nact == 0) {
                 converged = true;
