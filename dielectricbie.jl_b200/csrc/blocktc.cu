@@ -176,42 +176,53 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
     lo = pack_bf16(a - ah, b - bh);
 }
 
-// One thread's half row of a chunk's kernel tile: 32 sources (groups gq0..gq0+3).
-// AX = 0/1/2: the rows of this warp have normal +-e_AX (sign applied in the
-// epilogue); AX = 3: general normal.
+// One thread's half row of a chunk's kernel tile: 32 sources (groups gq0..gq0+3),
+// processed 16 at a time. AX = 0/1/2: the rows of this warp have normal +-e_AX
+// (sign applied in the epilogue); AX = 3: general normal.
 template <int AX>
-__device__ __forceinline__ void gen_half_row(const float4* __restrict__ cs, float xi, float yi, float zi, float n0,
+__device__ __forceinline__ void gen_half_row(const float* __restrict__ cs, float xi, float yi, float zi, float n0,
                                              float n1, float n2, int gq0, bool self, int64_t j0, int64_t i,
                                              uint8_t* Ah, uint8_t* Al, uint32_t row_off, uint32_t rsw) {
 #pragma unroll 1
-    for (int gq = gq0; gq < gq0 + 4; ++gq) {
-        float v[8];
+    for (int gq = gq0; gq < gq0 + 4; gq += 2) {
+        float v[16];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const float4 c = cs[gq * 8 + e];
-            const float dx = xi - c.x, dy = yi - c.y, dz = zi - c.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float ri = rsqrt_mufu(r2);
-            float dn;
-            if (AX == 0) dn = dx;
-            else if (AX == 1) dn = dy;
-            else if (AX == 2) dn = dz;
-            else dn = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
-            v[e] = (dn * ri) * (ri * ri);
+        for (int e4 = 0; e4 < 4; ++e4) {
+            const int b = gq * 8 + e4 * 4;
+            const float4 X4 = *reinterpret_cast<const float4*>(cs + b);
+            const float4 Y4 = *reinterpret_cast<const float4*>(cs + KC + b);
+            const float4 Z4 = *reinterpret_cast<const float4*>(cs + 2 * KC + b);
+            const float sx[4] = {X4.x, X4.y, X4.z, X4.w}, sy[4] = {Y4.x, Y4.y, Y4.z, Y4.w},
+                        sz[4] = {Z4.x, Z4.y, Z4.z, Z4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float dx = xi - sx[e], dy = yi - sy[e], dz = zi - sz[e];
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float ri = rsqrt_mufu(r2);
+                float dn;
+                if (AX == 0) dn = dx;
+                else if (AX == 1) dn = dy;
+                else if (AX == 2) dn = dz;
+                else dn = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+                v[e4 * 4 + e] = (dn * ri) * (ri * ri);
+            }
         }
         if (self) {
 #pragma unroll
-            for (int e = 0; e < 8; ++e)
+            for (int e = 0; e < 16; ++e)
                 if (j0 + gq * 8 + e == i) v[e] = 0.f;
         }
-        uint4 h, l;
-        split2(v[0], v[1], h.x, l.x);
-        split2(v[2], v[3], h.y, l.y);
-        split2(v[4], v[5], h.z, l.z);
-        split2(v[6], v[7], h.w, l.w);
-        const uint32_t off = row_off + ((((uint32_t)gq) ^ rsw) << 4);
-        *reinterpret_cast<uint4*>(Ah + off) = h;
-        *reinterpret_cast<uint4*>(Al + off) = l;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            uint4 hi, lo;
+            split2(v[8 * h + 0], v[8 * h + 1], hi.x, lo.x);
+            split2(v[8 * h + 2], v[8 * h + 3], hi.y, lo.y);
+            split2(v[8 * h + 4], v[8 * h + 5], hi.z, lo.z);
+            split2(v[8 * h + 6], v[8 * h + 7], hi.w, lo.w);
+            const uint32_t off = row_off + ((((uint32_t)(gq + h)) ^ rsw) << 4);
+            *reinterpret_cast<uint4*>(Ah + off) = hi;
+            *reinterpret_cast<uint4*>(Al + off) = lo;
+        }
     }
 }
 
@@ -224,11 +235,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     const uint32_t b_bytes = (uint32_t)npad * 128;  // one term of the B tile
     uint8_t* A = base;                               // [S][2][a_bytes]
     uint8_t* B = A + S * 2 * a_bytes;                // [S][2][b_bytes]
-    float4* crd = (float4*)(B + S * 2 * b_bytes);    // [S][KC]
-    uint64_t* full_a = (uint64_t*)(crd + S * KC);
+    float* crd = (float*)(B + S * 2 * b_bytes);      // [S][3][KC] source coordinates (SoA, FP32 relative)
+    uint64_t* full_a = (uint64_t*)(crd + S * 3 * KC);
     uint64_t* full_b = full_a + S;
     uint64_t* empty = full_b + S;
-    uint64_t* acc_done = empty + S;
+    uint64_t* crd_full = empty + S;
+    uint64_t* acc_done = crd_full + S;
     uint32_t* tmem_slot = (uint32_t*)(acc_done + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
@@ -245,6 +257,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             mbar_init(&full_a[s], NGEN);
             mbar_init(&full_b[s], 1);
             mbar_init(&empty[s], 1);
+            mbar_init(&crd_full[s], 32);
         }
         mbar_init(acc_done, 1);
         *abort_flag = 0;
@@ -296,20 +309,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             const int s = lc % S;
             const uint32_t u = (uint32_t)(lc / S);
             const int64_t j0 = (ch0 + lc) * KC;
-            if (threadIdx.x < KC) {
-                const int64_t j = j0 + threadIdx.x;
-                float4 c;
-                if (j < n)
-                    c = make_float4((float)(P.g.x[j] - ox), (float)(P.g.y[j] - oy), (float)(P.g.z[j] - oz), 0.f);
-                else
-                    c = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.f);  // padded source: G underflows to 0
-                crd[s * KC + threadIdx.x] = c;
-            }
-            bool fail = (lc >= S) && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag);
-            if (gen_any(fail)) break;  // uniform exit; the barrier also publishes crd[s]
+            // coordinates staged (and stage s released by the MMAs of chunk lc - S)
+            if (!mbar_wait(&crd_full[s], u & 1, abort_flag)) break;
             uint8_t* Ah = A + (s * 2 + 0) * a_bytes;
             uint8_t* Al = A + (s * 2 + 1) * a_bytes;
-            const float4* cs = crd + s * KC;
+            const float* cs = crd + s * 3 * KC;
             const bool self = (j0 < i0 + M) && (j0 + KC > i0);
             const int gq0 = half * 4;
             switch (ax) {
@@ -371,22 +375,36 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
         }
         __syncwarp();
     } else {
-        // ------------------------- Q-tile producer ---------------------------
-        if (lane == 0) {
-            const uint32_t bytes = 2 * b_bytes;
-            int issued = 0;
-            for (int lc = 0; lc < nch; ++lc) {
-                const int s = lc % S;
-                const uint32_t u = (uint32_t)(lc / S);
-                if (lc >= S && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag)) break;
+        // ------------- Q-tile and source-coordinate producer -----------------
+        const uint32_t bytes = 2 * b_bytes;
+        int issued = 0;
+        for (int lc = 0; lc < nch; ++lc) {
+            const int s = lc % S;
+            const uint32_t u = (uint32_t)(lc / S);
+            if (lc >= S && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag)) break;
+            if (lane == 0) {
                 mbar_arrive_tx(&full_b[s], bytes);
                 bulk_g2s(B + s * 2 * b_bytes, P.bpack + (size_t)(ch0 + lc) * bytes, bytes, &full_b[s]);
                 issued = lc + 1;
             }
-            // on abort, wait for the copies still in flight (at most one per stage)
-            if (*abort_flag)
-                for (int lc = issued > S ? issued - S : 0; lc < issued; ++lc) mbar_wait_raw(&full_b[lc % S], (lc / S) & 1);
+            // source coordinates of the chunk, FP32 relative to the tile origin
+            float* cs = crd + s * 3 * KC;
+            const int64_t j0 = (ch0 + lc) * KC;
+#pragma unroll
+            for (int h = 0; h < KC / 32; ++h) {
+                const int t = lane + 32 * h;
+                const int64_t j = j0 + t;
+                float x = 1.0e18f, y = 1.0e18f, z = 1.0e18f;  // padded source: G underflows to 0
+                if (j < n) {
+                    x = (float)(P.g.x[j] - ox); y = (float)(P.g.y[j] - oy); z = (float)(P.g.z[j] - oz);
+                }
+                cs[t] = x; cs[KC + t] = y; cs[2 * KC + t] = z;
+            }
+            mbar_arrive(&crd_full[s]);
         }
+        // on abort, wait for the copies still in flight (at most one per stage)
+        if (lane == 0 && *abort_flag)
+            for (int lc = issued > S ? issued - S : 0; lc < issued; ++lc) mbar_wait_raw(&full_b[lc % S], (lc / S) & 1);
         __syncwarp();
     }
 
@@ -432,8 +450,8 @@ __global__ void k_pack_q(GeomDev g, const double* __restrict__ X, int ldx, int c
 
 size_t smem_bytes(int npad) {
     size_t a = (size_t)S * 2 * M * 128, b = (size_t)S * 2 * npad * 128;
-    size_t c = (size_t)S * KC * sizeof(float4);
-    size_t bars = (3 * S + 1) * sizeof(uint64_t) + 16;
+    size_t c = (size_t)S * 3 * KC * sizeof(float);
+    size_t bars = (4 * S + 1) * sizeof(uint64_t) + 16;
     return 1024 + a + b + c + bars;
 }
 

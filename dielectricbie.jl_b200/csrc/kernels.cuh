@@ -268,11 +268,12 @@ __global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int
 // K4 + K5, block-row form: one CTA per target panel P (nb consecutive rows).
 // Each block (P, Q) of the row is staged once in shared memory together with the
 // nb x kt slab of (p X)[Q rows] it multiplies, so block values and source slabs
-// are read once per panel (coalesced, 128-bit where aligned) instead of once per
-// output. Then Y[i][c] = (1/4pi) sum_s part[s][i][c] + sum_b B . X + t_i p_i X[i][c]
-// for the panel's rows, columns processed in tiles of at most kKT.
-constexpr int kKT = 64;         // column tile of the block-row combine
-constexpr int kCombOut = 16;    // outputs per thread (nb * kt <= blockDim * kCombOut)
+// are read once per panel instead of once per output. Thread t owns column
+// c = t % kt and the rows [g R, g R + R) of group g = t / kt: every slab value it
+// loads feeds R FMAs, and the R block values are warp-wide broadcasts. Then
+//   Y[i][c] = (1/4pi) sum_s part[s][i][c] + sum_b B . (p X) + t_i p_i X[i][c].
+constexpr int kKT = 64;     // column tile of the block-row combine
+constexpr int kRmax = 16;   // rows per thread (nb <= (256 / kt) * kRmax)
 __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const double* __restrict__ part, int nsplit,
                                                        const double* __restrict__ X, const double* __restrict__ pre,
                                                        const double* __restrict__ diag,
@@ -290,44 +291,48 @@ __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const d
     const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
     for (int c0 = 0; c0 < k; c0 += kKT) {
         const int kt = min(kKT, k - c0);
-        const int nout = nb * kt;
-        double acc[kCombOut];
+        const int G = (int)blockDim.x / kt;
+        const int R = (nb + G - 1) / G;
+        const int c = threadIdx.x % kt, grp = threadIdx.x / kt;
+        const bool act = grp < G;
+        const int r0 = grp * R;
+        double acc[kRmax];
 #pragma unroll
-        for (int m = 0; m < kCombOut; ++m) acc[m] = 0.0;
+        for (int m = 0; m < kRmax; ++m) acc[m] = 0.0;
         for (int b = b0; b < b1; ++b) {
             __syncthreads();
             const double* vb = val + (int64_t)b * nb2;
             for (int e = threadIdx.x; e < nb2; e += blockDim.x) sv[e] = vb[e];
             const int64_t base = (int64_t)col[b] * nb;
-            for (int e = threadIdx.x; e < nout; e += blockDim.x) {
-                const int q = e / kt, c = e - q * kt;
-                double x = X[(base + q) * k + c0 + c];
+            for (int e = threadIdx.x; e < nb * kt; e += blockDim.x) {
+                const int q = e / kt, cc = e - q * kt;
+                const double x = X[(base + q) * k + c0 + cc];
                 sx[e] = pre ? pre[base + q] * x : x;
             }
             __syncthreads();
+            if (act) {
+                for (int q = 0; q < nb; ++q) {
+                    const double x = sx[q * kt + c];
+                    const double* v = sv + q * nb + r0;
 #pragma unroll
-            for (int m = 0; m < kCombOut; ++m) {
-                const int o = threadIdx.x + m * blockDim.x;
-                if (o < nout) {
-                    const int r = o / kt, c = o - r * kt;
-                    double a = acc[m];
-                    for (int q = 0; q < nb; ++q) a = fma(sv[q * nb + r], sx[q * kt + c], a);
-                    acc[m] = a;
+                    for (int m = 0; m < kRmax; ++m)
+                        if (m < R && r0 + m < nb) acc[m] = fma(v[m], x, acc[m]);
                 }
             }
         }
+        if (act) {
 #pragma unroll
-        for (int m = 0; m < kCombOut; ++m) {
-            const int o = threadIdx.x + m * blockDim.x;
-            if (o < nout) {
-                const int r = o / kt, c = o - r * kt;
-                const int64_t i = row0 + r;
-                const int64_t e = i * k + c0 + c;
-                double s = 0.0;
-                for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
-                s = s * kInv4Pi + acc[m];
-                if (diag) s += diag[i] * (pre ? pre[i] : 1.0) * X[e];
-                Y[e] = s;
+            for (int m = 0; m < kRmax; ++m) {
+                const int r = r0 + m;
+                if (m < R && r < nb) {
+                    const int64_t i = row0 + r;
+                    const int64_t e = i * k + c0 + c;
+                    double s = 0.0;
+                    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
+                    s = s * kInv4Pi + acc[m];
+                    if (diag) s += diag[i] * (pre ? pre[i] : 1.0) * X[e];
+                    Y[e] = s;
+                }
             }
         }
     }

@@ -288,7 +288,7 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
                                 : 0.0) +
                           (double)g->n * k * 8 * (2 + sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
     Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
-    if (g->nb > 0 && (int64_t)g->npanels * g->nb == g->n && (int64_t)g->nb * std::min(k, kKT) <= 256 * kCombOut) {
+    if (g->nb > 0 && (int64_t)g->npanels * g->nb == g->n && (g->nb + (256 / std::min(k, kKT)) - 1) / (256 / std::min(k, kKT)) <= kRmax) {
         const size_t sm = sizeof(double) * ((size_t)g->nb * g->nb + (size_t)g->nb * std::min(k, kKT));
         static bool attr = false;
         if (!attr) {
