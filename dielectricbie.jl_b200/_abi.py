@@ -14,9 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbie_b200.so")
 
 BIE_OK, BIE_EINVAL, BIE_ENOMEM, BIE_ECUDA, BIE_ENOCONV, BIE_ETIMEOUT, BIE_EUNSUPPORTED, BIE_ENODEVICE = range(8)
-BIE_FP64, BIE_FP32, BIE_BF16X3 = 0, 1, 2
+BIE_FP64, BIE_FP32, BIE_BF16X3, BIE_BF16X6 = 0, 1, 2, 3
 BIE_NO_CORRECTIONS, BIE_NO_DIAG, BIE_NO_VERIFY = 1, 2, 4
-PRECISIONS = {"fp64": BIE_FP64, "fp32": BIE_FP32, "bf16x3": BIE_BF16X3}
+PRECISIONS = {"fp64": BIE_FP64, "fp32": BIE_FP32, "bf16x3": BIE_BF16X3, "bf16x6": BIE_BF16X6}
 
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTS = [

@@ -169,20 +169,28 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
     return *reinterpret_cast<uint32_t*>(&h);
 }
 
-// Split two FP32 values into packed bf16 hi and lo words.
-__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
-    hi = pack_bf16(a, b);
-    float ah = __uint_as_float(hi << 16), bh = __uint_as_float(hi & 0xFFFF0000u);
-    lo = pack_bf16(a - ah, b - bh);
+// Split two FP32 values into NP packed bf16 pieces (hi, lo or hi, mid, lo): each
+// piece is the bf16 rounding of what the previous pieces leave.
+template <int NP>
+__device__ __forceinline__ void split_pieces(float a, float b, uint32_t* out) {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const uint32_t w = pack_bf16(a, b);
+        out[p] = w;
+        if (p + 1 < NP) {
+            a -= __uint_as_float(w << 16);
+            b -= __uint_as_float(w & 0xFFFF0000u);
+        }
+    }
 }
 
 // One thread's half row of a chunk's kernel tile: 32 sources (groups gq0..gq0+3),
 // processed 16 at a time. AX = 0/1/2: the rows of this warp have normal +-e_AX
 // (sign applied in the epilogue); AX = 3: general normal.
-template <int AX>
+template <int AX, int NP>
 __device__ __forceinline__ void gen_half_row(const float* __restrict__ cs, float xi, float yi, float zi, float n0,
                                              float n1, float n2, int gq0, bool self, int64_t j0, int64_t i,
-                                             uint8_t* Ah, uint8_t* Al, uint32_t row_off, uint32_t rsw) {
+                                             uint8_t* Astage, uint32_t a_bytes, uint32_t row_off, uint32_t rsw) {
 #pragma unroll 1
     for (int gq = gq0; gq < gq0 + 4; gq += 2) {
         float v[16];
@@ -214,18 +222,18 @@ __device__ __forceinline__ void gen_half_row(const float* __restrict__ cs, float
         }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            uint4 hi, lo;
-            split2(v[8 * h + 0], v[8 * h + 1], hi.x, lo.x);
-            split2(v[8 * h + 2], v[8 * h + 3], hi.y, lo.y);
-            split2(v[8 * h + 4], v[8 * h + 5], hi.z, lo.z);
-            split2(v[8 * h + 6], v[8 * h + 7], hi.w, lo.w);
+            uint32_t w[4][NP];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) split_pieces<NP>(v[8 * h + 2 * e], v[8 * h + 2 * e + 1], w[e]);
             const uint32_t off = row_off + ((((uint32_t)(gq + h)) ^ rsw) << 4);
-            *reinterpret_cast<uint4*>(Ah + off) = hi;
-            *reinterpret_cast<uint4*>(Al + off) = lo;
+#pragma unroll
+            for (int p = 0; p < NP; ++p)
+                *reinterpret_cast<uint4*>(Astage + p * a_bytes + off) = make_uint4(w[0][p], w[1][p], w[2][p], w[3][p]);
         }
     }
 }
 
+template <int NP>
 __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // carve-up aligned to 1024 bytes in the shared window (128-byte swizzle atoms)
@@ -233,9 +241,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     const int npad = P.npad;
     const uint32_t a_bytes = M * 128;          // one term of the A tile (16 KB)
     const uint32_t b_bytes = (uint32_t)npad * 128;  // one term of the B tile
-    uint8_t* A = base;                               // [S][2][a_bytes]
-    uint8_t* B = A + S * 2 * a_bytes;                // [S][2][b_bytes]
-    float* crd = (float*)(B + S * 2 * b_bytes);      // [S][3][KC] source coordinates (SoA, FP32 relative)
+    uint8_t* A = base;                               // [S][NP][a_bytes]
+    uint8_t* B = A + S * NP * a_bytes;               // [S][NP][b_bytes]
+    float* crd = (float*)(B + S * NP * b_bytes);     // [S][3][KC] source coordinates (SoA, FP32 relative)
     uint64_t* full_a = (uint64_t*)(crd + S * 3 * KC);
     uint64_t* full_b = full_a + S;
     uint64_t* empty = full_b + S;
@@ -311,16 +319,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             const int64_t j0 = (ch0 + lc) * KC;
             // coordinates staged (and stage s released by the MMAs of chunk lc - S)
             if (!mbar_wait(&crd_full[s], u & 1, abort_flag)) break;
-            uint8_t* Ah = A + (s * 2 + 0) * a_bytes;
-            uint8_t* Al = A + (s * 2 + 1) * a_bytes;
+            uint8_t* As = A + s * NP * a_bytes;
             const float* cs = crd + s * 3 * KC;
             const bool self = (j0 < i0 + M) && (j0 + KC > i0);
             const int gq0 = half * 4;
             switch (ax) {
-                case 0: gen_half_row<0>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
-                case 1: gen_half_row<1>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
-                case 2: gen_half_row<2>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
-                default: gen_half_row<3>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, Ah, Al, row_off, rsw); break;
+                case 0: gen_half_row<0, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
+                case 1: gen_half_row<1, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
+                case 2: gen_half_row<2, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
+                default: gen_half_row<3, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&full_a[s]);
@@ -358,14 +365,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
                 if (!mbar_wait(&full_a[s], u & 1, abort_flag)) break;
                 if (!mbar_wait(&full_b[s], u & 1, abort_flag)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t ah = smem_u32(A + (s * 2 + 0) * a_bytes), al = smem_u32(A + (s * 2 + 1) * a_bytes);
-                const uint32_t bh = smem_u32(B + (s * 2 + 0) * b_bytes), bl = smem_u32(B + (s * 2 + 1) * b_bytes);
+                const uint32_t a0 = smem_u32(A + s * NP * a_bytes), b0 = smem_u32(B + s * NP * b_bytes);
+                // products of pieces whose orders sum to at most NP - 1
 #pragma unroll
                 for (int kk = 0; kk < KC / 16; ++kk) {
                     const uint32_t ko = (uint32_t)kk * 32u;
-                    mma_bf16(tmem, sw128_desc(ah + ko), sw128_desc(bh + ko), idesc, (lc > 0 || kk > 0) ? 1u : 0u);
-                    mma_bf16(tmem, sw128_desc(ah + ko), sw128_desc(bl + ko), idesc, 1u);
-                    mma_bf16(tmem, sw128_desc(al + ko), sw128_desc(bh + ko), idesc, 1u);
+                    bool first = (lc == 0 && kk == 0);
+#pragma unroll
+                    for (int pa = 0; pa < NP; ++pa)
+#pragma unroll
+                        for (int pb = 0; pb + pa < NP; ++pb) {
+                            mma_bf16(tmem, sw128_desc(a0 + pa * a_bytes + ko), sw128_desc(b0 + pb * b_bytes + ko), idesc,
+                                     first ? 0u : 1u);
+                            first = false;
+                        }
                 }
                 mma_commit(&empty[s]);
             }
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
         __syncwarp();
     } else {
         // ------------- Q-tile and source-coordinate producer -----------------
-        const uint32_t bytes = 2 * b_bytes;
+        const uint32_t bytes = NP * b_bytes;
         int issued = 0;
         for (int lc = 0; lc < nch; ++lc) {
             const int s = lc % S;
@@ -384,7 +397,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             if (lc >= S && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag)) break;
             if (lane == 0) {
                 mbar_arrive_tx(&full_b[s], bytes);
-                bulk_g2s(B + s * 2 * b_bytes, P.bpack + (size_t)(ch0 + lc) * bytes, bytes, &full_b[s]);
+                bulk_g2s(B + s * NP * b_bytes, P.bpack + (size_t)(ch0 + lc) * bytes, bytes, &full_b[s]);
                 issued = lc + 1;
             }
             // source coordinates of the chunk, FP32 relative to the tile origin
@@ -416,9 +429,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     }
 }
 
-// Packs Q(j, c) = w_j p_j X[j][c0 + c] as bf16 hi/lo, in the swizzled K-major
-// smem image of each 64-source chunk: [chunk][term][row c][128 B]. Rows c >= keff
+// Packs Q(j, c) = w_j p_j X[j][c0 + c] as NP bf16 pieces, in the swizzled K-major
+// smem image of each 64-source chunk: [chunk][piece][row c][128 B]. Rows c >= keff
 // and sources j >= n are zero.
+template <int NP>
 __global__ void k_pack_q(GeomDev g, const double* __restrict__ X, int ldx, int c0, int keff,
                          const double* __restrict__ pre, int npad, int64_t nchunks, uint8_t* __restrict__ out) {
     // one thread per (chunk, row c, 8-source group)
@@ -436,38 +450,33 @@ __global__ void k_pack_q(GeomDev g, const double* __restrict__ X, int ldx, int c
         if (j < g.n && c < keff) val = g.w[j] * (pre ? pre[j] : 1.0) * X[j * ldx + c0 + c];
         v[q] = (float)val;
     }
-    uint4 h, l;
-    split2(v[0], v[1], h.x, l.x);
-    split2(v[2], v[3], h.y, l.y);
-    split2(v[4], v[5], h.z, l.z);
-    split2(v[6], v[7], h.w, l.w);
+    uint32_t w[4][NP];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) split_pieces<NP>(v[2 * q], v[2 * q + 1], w[q]);
     const size_t tile = (size_t)npad * 128;
-    uint8_t* base = out + (size_t)ch * 2 * tile;
+    uint8_t* base = out + (size_t)ch * NP * tile;
     const uint32_t off = (uint32_t)c * 128u + ((((uint32_t)gq) ^ (uint32_t)(c & 7)) << 4);
-    *reinterpret_cast<uint4*>(base + off) = h;
-    *reinterpret_cast<uint4*>(base + tile + off) = l;
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+        *reinterpret_cast<uint4*>(base + p * tile + off) = make_uint4(w[0][p], w[1][p], w[2][p], w[3][p]);
 }
 
-size_t smem_bytes(int npad) {
-    size_t a = (size_t)S * 2 * M * 128, b = (size_t)S * 2 * npad * 128;
+size_t smem_bytes(int npad, int np) {
+    size_t a = (size_t)S * np * M * 128, b = (size_t)S * np * npad * 128;
     size_t c = (size_t)S * 3 * KC * sizeof(float);
     size_t bars = (4 * S + 1) * sizeof(uint64_t) + 16;
     return 1024 + a + b + c + bars;
 }
 
-}  // namespace tc
-
-int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
-
-// Runs K3 for columns [c0, c0 + kc) (kc <= 256) of X into part[s][i][c0 + c].
-void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
-                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s) {
-    const int npad = tc_npad(kc);
-    const int64_t nchunks = (g.n + tc::KC - 1) / tc::KC;
+template <int NP>
+void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit, int64_t cps,
+               double* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s) {
+    const int npad = ((kc + 15) / 16) * 16;
+    const int64_t nchunks = (g.n + KC - 1) / KC;
     const int64_t pk = nchunks * npad * 8;
-    tc::k_pack_q<<<(unsigned)((pk + 255) / 256), 256, 0, s>>>(g, X, ldx, c0, kc, pre, npad, nchunks, bpack);
+    k_pack_q<NP><<<(unsigned)((pk + 255) / 256), 256, 0, s>>>(g, X, ldx, c0, kc, pre, npad, nchunks, bpack);
     BIE_CK(cudaGetLastError());
-    tc::Params P;
+    Params P;
     P.g = g;
     P.bpack = bpack;
     P.npad = npad;
@@ -478,24 +487,39 @@ void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc,
     P.ldp = ldp;
     P.c0 = c0;
     P.err = err;
-    const size_t sm = tc::smem_bytes(npad);
+    const size_t sm = smem_bytes(npad, NP);
     static size_t configured = 0;
     if (sm > configured) {
-        BIE_CK(cudaFuncSetAttribute(tc::k_dt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        BIE_CK(cudaFuncSetAttribute(k_dt_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         configured = sm;
     }
-    dim3 grid((unsigned)((g.n + tc::M - 1) / tc::M), (unsigned)nsplit);
-    tc::k_dt_tc<<<grid, tc::NTHREADS, sm, s>>>(P);
+    dim3 grid((unsigned)((g.n + M - 1) / M), (unsigned)nsplit);
+    k_dt_tc<NP><<<grid, NTHREADS, sm, s>>>(P);
     BIE_CK(cudaGetLastError());
 }
 
-size_t block_tc_pack_bytes(int64_t n, int kc) {
-    const int64_t nchunks = (n + tc::KC - 1) / tc::KC;
-    return (size_t)nchunks * 2 * tc_npad(kc) * 128;
+}  // namespace tc
+
+int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
+
+// Runs K3 for columns [c0, c0 + kc) (kc <= 256) of X into part[s][i][c0 + c],
+// with the kernel and right-hand sides split into `pieces` (2: three products,
+// 3: six products) bf16 pieces.
+void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
+                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, int pieces, cudaStream_t s) {
+    if (pieces == 3)
+        tc::launch_tc<3>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, s);
+    else
+        tc::launch_tc<2>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, s);
 }
 
-int block_tc_ctas_per_sm(int kc) {
-    const size_t sm = tc::smem_bytes(tc_npad(kc));
+size_t block_tc_pack_bytes(int64_t n, int kc, int pieces) {
+    const int64_t nchunks = (n + tc::KC - 1) / tc::KC;
+    return (size_t)nchunks * pieces * tc_npad(kc) * 128;
+}
+
+int block_tc_ctas_per_sm(int kc, int pieces) {
+    const size_t sm = tc::smem_bytes(tc_npad(kc), pieces);
     return std::max(1, (int)((227 * 1024) / (sm + 1024)));
 }
 

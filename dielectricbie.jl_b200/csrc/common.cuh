@@ -24,12 +24,16 @@ struct GeomDev {
     int64_t n;
 };
 
-// K3 (blocktc.cu): tensor-core block direct sum for columns [c0, c0 + kc), kc <= 256.
+// K3 (blocktc.cu): tensor-core block direct sum for columns [c0, c0 + kc), kc <= 256,
+// kernel and right-hand sides split into `pieces` bf16 pieces (2 or 3).
 void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
-                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s);
-size_t block_tc_pack_bytes(int64_t n, int kc);
-int block_tc_ctas_per_sm(int kc);
+                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, int pieces, cudaStream_t s);
+size_t block_tc_pack_bytes(int64_t n, int kc, int pieces);
+int block_tc_ctas_per_sm(int kc, int pieces);
 int tc_npad(int kc);
+// K1 with the FP64 tensor-core contraction (dt64mma.cu), columns [c0, c0 + kc), kc <= 64.
+void launch_dt_f64_mma(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
+                       int64_t chunk, double* part, int ldp, cudaStream_t s);
 constexpr int kTcTileM = 128;   // targets per tensor-core tile
 constexpr int kTcChunk = 64;    // sources per tensor-core chunk
 

@@ -274,6 +274,7 @@ __global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int
 //   Y[i][c] = (1/4pi) sum_s part[s][i][c] + sum_b B . (p X) + t_i p_i X[i][c].
 constexpr int kKT = 64;     // column tile of the block-row combine
 constexpr int kRmax = 16;   // rows per thread (nb <= (256 / kt) * kRmax)
+template <int R>
 __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const double* __restrict__ part, int nsplit,
                                                        const double* __restrict__ X, const double* __restrict__ pre,
                                                        const double* __restrict__ diag,
@@ -285,24 +286,28 @@ __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const d
     const int P = blockIdx.x;
     const int64_t row0 = (int64_t)P * nb;
     const int nb2 = nb * nb;
-    double* sv = smc;          // [nb][nb], column-major block (sv[q * nb + r])
-    double* sx = smc + nb2;    // [nb][kt]
     const int64_t tot = n * (int64_t)k;
     const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
     for (int c0 = 0; c0 < k; c0 += kKT) {
         const int kt = min(kKT, k - c0);
         const int G = (int)blockDim.x / kt;
-        const int R = (nb + G - 1) / G;
         const int c = threadIdx.x % kt, grp = threadIdx.x / kt;
-        const bool act = grp < G;
         const int r0 = grp * R;
-        double acc[kRmax];
+        // rows of this thread: r0 .. r0 + R - 1, valid while < nb (sv is padded to a multiple of R rows)
+        const bool act = grp < G && r0 < nb;
+        const int ldv = ((nb + R - 1) / R) * R;  // padded leading dimension of the staged block
+        double* sv = smc;           // [nb][ldv], sv[q * ldv + r]
+        double* sx = smc + nb * ldv;  // [nb][kt]
+        double acc[R];
 #pragma unroll
-        for (int m = 0; m < kRmax; ++m) acc[m] = 0.0;
+        for (int m = 0; m < R; ++m) acc[m] = 0.0;
         for (int b = b0; b < b1; ++b) {
             __syncthreads();
             const double* vb = val + (int64_t)b * nb2;
-            for (int e = threadIdx.x; e < nb2; e += blockDim.x) sv[e] = vb[e];
+            for (int e = threadIdx.x; e < nb * ldv; e += blockDim.x) {
+                const int q = e / ldv, r = e - q * ldv;
+                sv[e] = r < nb ? vb[q * nb + r] : 0.0;
+            }
             const int64_t base = (int64_t)col[b] * nb;
             for (int e = threadIdx.x; e < nb * kt; e += blockDim.x) {
                 const int q = e / kt, cc = e - q * kt;
@@ -311,20 +316,20 @@ __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const d
             }
             __syncthreads();
             if (act) {
+#pragma unroll 4
                 for (int q = 0; q < nb; ++q) {
                     const double x = sx[q * kt + c];
-                    const double* v = sv + q * nb + r0;
+                    const double* v = sv + q * ldv + r0;
 #pragma unroll
-                    for (int m = 0; m < kRmax; ++m)
-                        if (m < R && r0 + m < nb) acc[m] = fma(v[m], x, acc[m]);
+                    for (int m = 0; m < R; ++m) acc[m] = fma(v[m], x, acc[m]);
                 }
             }
         }
         if (act) {
 #pragma unroll
-            for (int m = 0; m < kRmax; ++m) {
+            for (int m = 0; m < R; ++m) {
                 const int r = r0 + m;
-                if (m < R && r < nb) {
+                if (r < nb) {
                     const int64_t i = row0 + r;
                     const int64_t e = i * k + c0 + c;
                     double s = 0.0;

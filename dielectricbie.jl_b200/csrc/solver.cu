@@ -40,9 +40,11 @@ struct bie_geom {
 namespace bie {
 
 // Relative errors of the reduced-precision operators (measured on the config boxes:
-// ~4e-6 for the split-BF16 three-term contraction, ~1e-7 for the FP32 direct sum),
+// ~4e-6 for the split-BF16 three-term contraction, ~1e-7 for the six-term one and
+// the FP32 direct sum),
 // used to decide when a residual update may run in reduced precision.
 constexpr double kDeltaBF16X3 = 4e-6;
+constexpr double kDeltaBF16X6 = 3e-7;
 constexpr double kDeltaFP32 = 3e-7;
 
 namespace {
@@ -218,6 +220,18 @@ int pick_C(int rem) {
 Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const double* pre, const double* T,
                  int64_t M, cudaStream_t s) {
     GeomDev gd = gdev(g);
+    if (kind == Kern::DT64 && k >= 8) {
+        // FP64 tensor-core contraction, 64 columns per launch, 2 CTAs of 128 targets per SM
+        Split sp = choose_split(g->n, g->n, g->sms, 2);
+        g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
+        const double npairs = (double)g->n * (g->n - 1);
+        for (int c0 = 0; c0 < k; c0 += 64) {
+            const int kc = std::min(64, k - c0);
+            Prof pf(g, BIE_KERNEL_DIRECT_FP64, s, 1, npairs, npairs * kc);
+            launch_dt_f64_mma(gd, X, ldx, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, s);
+        }
+        return sp;
+    }
     int64_t rows = kind == Kern::POT64 ? M : g->n;
     int Cmax = pick_C(k);
     Split sp = choose_split(rows, g->n, g->sms, occ_for(kind, Cmax));
@@ -245,10 +259,10 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
 
 // K3 launch plan: enough source splits for >= 2 waves of CTAs, and at most 256
 // chunks (16384 sources) accumulated in FP32 tensor memory per FP64 partial.
-Split tc_split(const bie_geom* g, int kc) {
+Split tc_split(const bie_geom* g, int kc, int pieces) {
     const int64_t tiles = (g->n + kTcTileM - 1) / kTcTileM;
     const int64_t chunks = (g->n + kTcChunk - 1) / kTcChunk;
-    const int64_t slots = (int64_t)g->sms * block_tc_ctas_per_sm(kc);
+    const int64_t slots = (int64_t)g->sms * block_tc_ctas_per_sm(kc, pieces);
     int64_t ns = std::max<int64_t>(1, (2 * slots + tiles - 1) / tiles);
     ns = std::max<int64_t>(ns, (chunks + 255) / 256);
     ns = std::min<int64_t>(ns, chunks);
@@ -257,17 +271,17 @@ Split tc_split(const bie_geom* g, int kc) {
     return Split{(int)ns, cps};
 }
 
-Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, cudaStream_t s) {
+Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, int pieces, cudaStream_t s) {
     GeomDev gd = gdev(g);
-    Split sp = tc_split(g, std::min(k, 256));
+    Split sp = tc_split(g, std::min(k, 256), pieces);
     g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
-    g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 256)));
+    g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 256), pieces));
     for (int c0 = 0; c0 < k; c0 += 256) {
         int kc = std::min(256, k - c0);
         const double npairs = (double)g->n * (g->n - 1);
         Prof pf(g, BIE_KERNEL_DIRECT_TC, s, 2, npairs, npairs * tc_npad(kc));
         launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, g->bpack.as<uint8_t>(),
-                        g->errflag.as<int>(), s);
+                        g->errflag.as<int>(), pieces, s);
     }
     return sp;
 }
@@ -276,10 +290,10 @@ Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, cuda
 void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
               cudaStream_t s) {
     Split sp;
-    if (prec == BIE_BF16X3 && k >= 16) {
-        sp = direct_sum_tc(g, X, k, pre, s);
+    if ((prec == BIE_BF16X3 || prec == BIE_BF16X6) && k >= 16) {
+        sp = direct_sum_tc(g, X, k, pre, prec == BIE_BF16X6 ? 3 : 2, s);
     } else {
-        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // BF16X3 with k < 16 runs the FP32 kernel
+        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // tensor-core precisions with k < 16 run FP32
         sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
     }
     const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
@@ -288,17 +302,58 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
                                 : 0.0) +
                           (double)g->n * k * 8 * (2 + sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
     Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
-    if (g->nb > 0 && (int64_t)g->npanels * g->nb == g->n && (g->nb + (256 / std::min(k, kKT)) - 1) / (256 / std::min(k, kKT)) <= kRmax) {
-        const size_t sm = sizeof(double) * ((size_t)g->nb * g->nb + (size_t)g->nb * std::min(k, kKT));
+    const int kt0 = std::min(k, kKT);
+    const int G0 = 256 / kt0;
+    const int R0 = (g->nb + G0 - 1) / G0;
+    if (g->nb > 0 && (int64_t)g->npanels * g->nb == g->n && R0 <= kRmax) {
+        // shared memory: the padded block (nb x G R) and the slab (nb x kt) of the widest tile
+        const size_t sm = sizeof(double) * ((size_t)g->nb * G0 * R0 + (size_t)g->nb * kt0);
         static bool attr = false;
         if (!attr) {
-            BIE_CK(cudaFuncSetAttribute(k_combine_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+            const void* fs[] = {(const void*)k_combine_panel<1>, (const void*)k_combine_panel<2>,
+                                (const void*)k_combine_panel<3>, (const void*)k_combine_panel<4>,
+                                (const void*)k_combine_panel<6>, (const void*)k_combine_panel<8>,
+                                (const void*)k_combine_panel<9>, (const void*)k_combine_panel<12>,
+                                (const void*)k_combine_panel<16>};
+            for (const void* f : fs)
+                BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
             attr = true;
         }
-        k_combine_panel<<<(unsigned)g->npanels, 256, sm, s>>>(
-            g->n, k, g->part.as<double>(), sp.nsplit, X, pre, dg ? g->diag.as<double>() : nullptr,
-            corr ? g->rowptr.as<int32_t>() : nullptr, corr ? g->col.as<int32_t>() : nullptr,
-            corr ? g->val.as<double>() : nullptr, g->nb, Y);
+        // the column tiles after the first are narrower or equal: the same R bound holds for them only if
+        // k is a multiple of kKT or k < kKT; otherwise fall through to the generic kernel
+        const bool uniform = k <= kKT || k % kKT == 0;
+        int Rk = R0 <= 1 ? 1 : R0 <= 2 ? 2 : R0 <= 3 ? 3 : R0 <= 4 ? 4 : R0 <= 6 ? 6 : R0 <= 8 ? 8 : R0 <= 9 ? 9
+                 : R0 <= 12 ? 12 : 16;
+        if (uniform) {
+            const double* dgp = dg ? g->diag.as<double>() : nullptr;
+            const int32_t* rp = corr ? g->rowptr.as<int32_t>() : nullptr;
+            const int32_t* cl = corr ? g->col.as<int32_t>() : nullptr;
+            const double* vl = corr ? g->val.as<double>() : nullptr;
+            const size_t ldv = (size_t)((g->nb + Rk - 1) / Rk) * Rk;
+            const size_t smr = sizeof(double) * ((size_t)g->nb * ldv + (size_t)g->nb * kt0);
+            (void)sm;
+#define BIE_COMB(RR)                                                                                            \
+    k_combine_panel<RR><<<(unsigned)g->npanels, 256, smr, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, pre, \
+                                                               dgp, rp, cl, vl, g->nb, Y)
+            switch (Rk) {
+                case 1: BIE_COMB(1); break;
+                case 2: BIE_COMB(2); break;
+                case 3: BIE_COMB(3); break;
+                case 4: BIE_COMB(4); break;
+                case 6: BIE_COMB(6); break;
+                case 8: BIE_COMB(8); break;
+                case 9: BIE_COMB(9); break;
+                case 12: BIE_COMB(12); break;
+                default: BIE_COMB(16); break;
+            }
+#undef BIE_COMB
+        } else {
+            k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
+                                                      dg ? g->diag.as<double>() : nullptr,
+                                                      corr ? g->rowptr.as<int32_t>() : nullptr,
+                                                      corr ? g->col.as<int32_t>() : nullptr,
+                                                      corr ? g->val.as<double>() : nullptr, g->nb, Y, k);
+        }
     } else {
         k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
                                                   dg ? g->diag.as<double>() : nullptr,
@@ -515,7 +570,8 @@ void check_device_error(bie_geom* g, cudaStream_t s) {
 }
 
 void check_prec(int prec) {
-    if (prec != BIE_FP64 && prec != BIE_FP32 && prec != BIE_BF16X3) throw Error(BIE_EINVAL, "unknown precision");
+    if (prec != BIE_FP64 && prec != BIE_FP32 && prec != BIE_BF16X3 && prec != BIE_BF16X6)
+        throw Error(BIE_EINVAL, "unknown precision");
 }
 
 }  // namespace
@@ -780,19 +836,31 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
         // reduced-precision operator (r -= A_low d): that update errs by about
         // delta * ||A d|| ~ delta * ||r||, delta being the operator's relative error,
         // which is admitted only while it stays below half the tolerance.
-        const double delta = o.precision == BIE_BF16X3 ? kDeltaBF16X3 : kDeltaFP32;
+        // Candidate operators for the residual update, cheapest first.
+        const bool tc_ok = k >= 16;
+        struct Upd { int prec; double delta; };
+        std::vector<Upd> upd;
+        if (o.precision == BIE_BF16X3 && tc_ok) upd.push_back({BIE_BF16X3, kDeltaBF16X3});
+        if ((o.precision == BIE_BF16X3 || o.precision == BIE_BF16X6) && tc_ok) upd.push_back({BIE_BF16X6, kDeltaBF16X6});
+        upd.push_back({BIE_FP32, kDeltaFP32});
         std::vector<double> rn = fn, eps_in(k);
         BIE_CK(cudaMemcpyAsync(rbuf, dF, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
         have_true_resid = true;
         for (int it_out = 0;; ++it_out) {
             int nact = 0;
-            bool lowp_update_ok = true;
+            int upd_prec = BIE_FP64;  // cheapest admissible reduced-precision update, else FP64
+            double worst = 0.0;       // max over active columns of ||r_c|| / tol_c
             for (int c = 0; c < k; ++c) {
                 act[c] = rn[c] > tol[c] ? 1 : 0;
                 nact += act[c];
                 rel[c] = fn[c] > 0 ? rn[c] / fn[c] : 0.0;
-                if (act[c] && delta * rn[c] > 0.5 * tol[c]) lowp_update_ok = false;
+                if (act[c]) worst = std::max(worst, rn[c] / tol[c]);
             }
+            for (const Upd& u : upd)
+                if (u.delta * worst <= 0.5) {
+                    upd_prec = u.prec;
+                    break;
+                }
             if (nact == 0) {
                 converged = true;
                 break;
@@ -811,9 +879,9 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             }
             BIE_CK(cudaGetLastError());
             ++outer;
-            if (lowp_update_ok) {
+            if (upd_prec != BIE_FP64) {
                 // r -= A_low d  (d = 0 in the frozen columns)
-                apply_op(g, g->dd.as<double>(), g->rr.as<double>(), k, o.precision, o.flags, nullptr, s);
+                apply_op(g, g->dd.as<double>(), g->rr.as<double>(), k, upd_prec, o.flags, nullptr, s);
                 ++lpmv;
                 Prof pf(g, BIE_KERNEL_KRYLOV, s);
                 k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, g->rr.as<double>(), 1.0, rbuf, n, k, nullptr);

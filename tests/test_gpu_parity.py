@@ -175,3 +175,26 @@ def test_solve_refined_bf16x3_vs_lu(bie, orc, cfg1, rng):
     assert st.solved and st.lowp_matvecs > 0
     for c in range(16):
         assert rel(X[:, c], X_lu[:, c]) < 1e-8
+
+
+def test_matvec_bf16x6_tensor_core(bie, cfg1, rng):
+    """Three bf16 pieces per operand, six products: FP32-level accuracy (residual updates)."""
+    itf = cfg1[0]
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-9, 1e-9, 8)
+    X = rng.standard_normal((itf.n, 32))
+    Y64 = op.mul(X)
+    Y6 = op.mul(X, precision="bf16x6")
+    Y3 = op.mul(X, precision="bf16x3")
+    assert rel(Y6, Y64) < 1e-6
+    assert rel(Y6, Y64) < 0.2 * rel(Y3, Y64)
+
+
+@pytest.mark.parametrize("k", [1, 3, 8, 64, 128])
+def test_combine_column_tiles(bie, cfg1, rng, k):
+    """Block-row correction apply for every column-tile shape (k < 64, k = 64, k multiple of 64)."""
+    itf, m, Cm, A = cfg1
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, 1e-9, 8)
+    X = rng.standard_normal((itf.n, k))
+    Y = op @ X
+    ref = A @ X + Cm @ X
+    assert rel(Y, ref) < 1e-13
