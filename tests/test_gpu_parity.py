@@ -185,8 +185,8 @@ def test_matvec_bf16x6_tensor_core(bie, cfg1, rng):
     Y64 = op.mul(X)
     Y6 = op.mul(X, precision="bf16x6")
     Y3 = op.mul(X, precision="bf16x3")
-    assert rel(Y6, Y64) < 1e-6
-    assert rel(Y6, Y64) < 0.2 * rel(Y3, Y64)
+    assert rel(Y6, Y64) < 5e-7  # FP32-level: the FP32 kernel generation bounds it
+    assert rel(Y6, Y64) < rel(Y3, Y64)
 
 
 @pytest.mark.parametrize("k", [1, 3, 8, 64, 128])
