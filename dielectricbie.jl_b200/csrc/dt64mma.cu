@@ -30,7 +30,7 @@ constexpr int TB = 128;   // targets per CTA
 constexpr int TSRC = 32;  // sources per shared-memory tile
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }
@@ -57,6 +57,7 @@ __device__ __forceinline__ void tile_step(const double* __restrict__ ssx, const 
                                           bool self, int64_t jt, const int64_t (&ti)[4]) {
     constexpr int LDQ = NC + 8;
     const int kq = lane & 3, grp = lane >> 2;
+#pragma unroll 2
     for (int k0 = 0; k0 < cnt; k0 += 4) {
         const int j = k0 + kq;
         const double sx = ssx[j], sy = ssy[j], sz = ssz[j];

@@ -282,39 +282,58 @@ __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const d
                                                        const int32_t* __restrict__ col,
                                                        const double* __restrict__ val, int nb,
                                                        double* __restrict__ Y) {
+    constexpr int PF = 16;  // staged elements per thread and array (nb <= 64, kt <= 64)
     extern __shared__ double smc[];
     const int P = blockIdx.x;
     const int64_t row0 = (int64_t)P * nb;
     const int nb2 = nb * nb;
     const int64_t tot = n * (int64_t)k;
     const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
+    const int T = blockDim.x;
     for (int c0 = 0; c0 < k; c0 += kKT) {
         const int kt = min(kKT, k - c0);
-        const int G = (int)blockDim.x / kt;
+        const int G = T / kt;
         const int c = threadIdx.x % kt, grp = threadIdx.x / kt;
         const int r0 = grp * R;
         // rows of this thread: r0 .. r0 + R - 1, valid while < nb (sv is padded to a multiple of R rows)
         const bool act = grp < G && r0 < nb;
         const int ldv = ((nb + R - 1) / R) * R;  // padded leading dimension of the staged block
-        double* sv = smc;           // [nb][ldv], sv[q * ldv + r]
-        double* sx = smc + nb * ldv;  // [nb][kt]
+        const int nv = nb * ldv, nxs = nb * kt;
+        double* sv = smc;        // [nb][ldv], sv[q * ldv + r]
+        double* sx = smc + nv;   // [nb][kt]
         double acc[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) acc[m] = 0.0;
-        for (int b = b0; b < b1; ++b) {
-            __syncthreads();
+        // register staging of one block: its values and the slab of (p X) it multiplies
+        double pv[PF], px[PF];
+        auto fetch = [&](int b) {
             const double* vb = val + (int64_t)b * nb2;
-            for (int e = threadIdx.x; e < nb * ldv; e += blockDim.x) {
-                const int q = e / ldv, r = e - q * ldv;
-                sv[e] = r < nb ? vb[q * nb + r] : 0.0;
-            }
             const int64_t base = (int64_t)col[b] * nb;
-            for (int e = threadIdx.x; e < nb * kt; e += blockDim.x) {
-                const int q = e / kt, cc = e - q * kt;
-                const double x = X[(base + q) * k + c0 + cc];
-                sx[e] = pre ? pre[base + q] * x : x;
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+                const int e = threadIdx.x + u * T;
+                if (e < nv) {
+                    const int q = e / ldv, r = e - q * ldv;
+                    pv[u] = r < nb ? vb[q * nb + r] : 0.0;
+                }
+                if (e < nxs) {
+                    const int q = e / kt, cc = e - q * kt;
+                    const double x = X[(base + q) * k + c0 + cc];
+                    px[u] = pre ? pre[base + q] * x : x;
+                }
+            }
+        };
+        if (b0 < b1) fetch(b0);
+        for (int b = b0; b < b1; ++b) {
+            __syncthreads();  // previous block consumed
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+                const int e = threadIdx.x + u * T;
+                if (e < nv) sv[e] = pv[u];
+                if (e < nxs) sx[e] = px[u];
             }
             __syncthreads();
+            if (b + 1 < b1) fetch(b + 1);  // next block's loads in flight during the math
             if (act) {
 #pragma unroll 4
                 for (int q = 0; q < nb; ++q) {
@@ -340,6 +359,7 @@ __global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const d
                 }
             }
         }
+        __syncthreads();  // smem reused by the next column tile
     }
 }
 

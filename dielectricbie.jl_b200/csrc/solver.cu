@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -305,7 +307,7 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
     const int kt0 = std::min(k, kKT);
     const int G0 = 256 / kt0;
     const int R0 = (g->nb + G0 - 1) / G0;
-    if (g->nb > 0 && (int64_t)g->npanels * g->nb == g->n && R0 <= kRmax) {
+    if (g->nb > 0 && g->nb <= 64 && (int64_t)g->npanels * g->nb == g->n && R0 <= kRmax) {
         // shared memory: the padded block (nb x G R) and the slab (nb x kt) of the widest tile
         const size_t sm = sizeof(double) * ((size_t)g->nb * G0 * R0 + (size_t)g->nb * kt0);
         static bool attr = false;
@@ -861,6 +863,12 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
                     upd_prec = u.prec;
                     break;
                 }
+            if (std::getenv("BIE_TRACE")) {
+                double mx = 0.0;
+                for (int c = 0; c < k; ++c) mx = std::max(mx, rel[c]);
+                std::fprintf(stderr, "[bie] outer %d: active %d, max |r|/|F| %.3e, worst |r|/tol %.3e, update %d\n",
+                             it_out, nact, mx, worst, upd_prec);
+            }
             if (nact == 0) {
                 converged = true;
                 break;
