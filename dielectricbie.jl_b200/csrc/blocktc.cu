@@ -283,15 +283,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     const uint32_t tmem = *tmem_slot;
 
     // tile origin: coordinates are rounded to FP32 relative to it
-    const int64_t io = min(i0, n - 1);
+    const int64_t io = P.g.perm[min(i0, n - 1)];
     const double ox = P.g.x[io], oy = P.g.y[io], oz = P.g.z[io];
 
     if (warp < NGEN / 32) {
         // ------------------------- generators -------------------------------
         const int r = threadIdx.x & (M - 1);  // tile row
         const int half = threadIdx.x / M;     // which 32 sources of each chunk
-        const int64_t i = i0 + r;
-        const bool valid = i < n;
+        const bool valid = i0 + r < n;
+        const int64_t i = valid ? (int64_t)P.g.perm[i0 + r] : n;  // original index of the target
         float xi, yi, zi, n0, n1, n2;
         if (valid) {
             xi = (float)(P.g.x[i] - ox); yi = (float)(P.g.y[i] - oy); zi = (float)(P.g.z[i] - oz);
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
             if (!mbar_wait(&crd_full[s], u & 1, abort_flag)) break;
             uint8_t* As = A + s * NP * a_bytes;
             const float* cs = crd + s * 3 * KC;
-            const bool self = (j0 < i0 + M) && (j0 + KC > i0);
+            const bool self = (i >= j0) && (i < j0 + KC);  // this chunk holds the target's own node
             const int gq0 = half * 4;
             switch (ax) {
                 case 0: gen_half_row<0, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;

@@ -22,6 +22,10 @@ struct GeomDev {
     const double *nx, *ny, *nz;  // node normals
     const double* w;             // quadrature weights
     int64_t n;
+    // Target order of the reduced-precision kernels: nodes sorted along a Morton
+    // curve, so that a 128-target tile is spatially compact and coordinates rounded
+    // to FP32 relative to the tile's first target stay accurate for near pairs.
+    const int32_t* perm;
 };
 
 // K3 (blocktc.cu): tensor-core block direct sum for columns [c0, c0 + kc), kc <= 256,

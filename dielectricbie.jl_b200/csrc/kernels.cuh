@@ -88,9 +88,10 @@ __global__ void __launch_bounds__(kTB) k_dt_f64(GeomDev g, const double* __restr
 
 // ---------------------------------------------------------------------------
 // K2: FP32 direct D^T sum with FP64 tile partials ("refined" inner operator).
-// Coordinates are shifted to the CTA's first target in FP64 before rounding to
-// FP32 (keeps near-pair differences accurate), rsqrt runs on the MUFU pipe,
-// each shared-memory tile accumulates in FP32 and is folded into FP64.
+// Targets are taken in the Morton order g.perm (compact tiles); coordinates are
+// shifted to the CTA's first target in FP64 before rounding to FP32 (keeps
+// near-pair differences accurate), rsqrt runs on the MUFU pipe, each
+// shared-memory tile accumulates in FP32 and is folded into FP64.
 // ---------------------------------------------------------------------------
 template <int C>
 __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restrict__ X, int ldx, int c0,
@@ -102,9 +103,9 @@ __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restr
     float* sz = sy + kTS;
     float* sq = sz + kTS;  // [kTS][C]
     const int64_t i0 = (int64_t)blockIdx.x * kTB;
-    const int64_t i = i0 + threadIdx.x;
-    const bool valid = i < g.n;
-    const int64_t io = min(i0, g.n - 1);
+    const bool valid = i0 + threadIdx.x < g.n;
+    const int64_t i = valid ? (int64_t)g.perm[i0 + threadIdx.x] : g.n;  // original index of the target
+    const int64_t io = g.perm[min(i0, g.n - 1)];
     const double ox = g.x[io], oy = g.y[io], oz = g.z[io];
     float xi = 0.f, yi = 0.f, zi = 0.f, n0 = 0.f, n1 = 0.f, n2 = 0.f;
     if (valid) {
@@ -131,29 +132,18 @@ __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restr
         float a32[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) a32[c] = 0.f;
-        const bool self_tile = (jt < i0 + kTB) && (jt + cnt > i0);
-        if (!self_tile) {
+        // The target's own node, if in this tile, has dx = dy = dz = 0 exactly (same
+        // FP64 value, same origin, same rounding); clamping r^2 keeps its r^-3 finite
+        // so it contributes exactly 0 (j != i exclusion without a branch).
 #pragma unroll 4
-            for (int t = 0; t < cnt; ++t) {
-                float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
-                float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                float ri = rsqrt_approx(r2);
-                float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
-                float gk = nd * ri * (ri * ri);
+        for (int t = 0; t < cnt; ++t) {
+            float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
+            float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-24f);
+            float ri = rsqrt_approx(r2);
+            float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+            float gk = (nd * ri) * (ri * ri);
 #pragma unroll
-                for (int c = 0; c < C; ++c) a32[c] = fmaf(gk, sq[t * C + c], a32[c]);
-            }
-        } else {
-            for (int t = 0; t < cnt; ++t) {
-                if (jt + t == i) continue;
-                float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
-                float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                float ri = rsqrt_approx(r2);
-                float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
-                float gk = nd * ri * (ri * ri);
-#pragma unroll
-                for (int c = 0; c < C; ++c) a32[c] = fmaf(gk, sq[t * C + c], a32[c]);
-            }
+            for (int c = 0; c < C; ++c) a32[c] = fmaf(gk, sq[t * C + c], a32[c]);
         }
 #pragma unroll
         for (int c = 0; c < C; ++c) acc[c] += (double)a32[c];

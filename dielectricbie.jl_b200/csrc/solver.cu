@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "kernels.cuh"
@@ -21,7 +22,7 @@ struct bie_geom {
     int32_t npanels = 0, nb = 0;
     int64_t nblocks = 0;
     size_t geom_bytes = 0;
-    bie::Buf x, y, z, nx, ny, nz, w, diag, pinv;
+    bie::Buf x, y, z, nx, ny, nz, w, diag, pinv, perm;
     bie::Buf rowptr, col, val;
     // operator workspace
     bie::Buf part, small, bpack, errflag;
@@ -126,7 +127,7 @@ struct Prof {
 
 GeomDev gdev(const bie_geom* g) {
     return GeomDev{g->x.as<double>(), g->y.as<double>(), g->z.as<double>(), g->nx.as<double>(),
-                   g->ny.as<double>(), g->nz.as<double>(), g->w.as<double>(), g->n};
+                   g->ny.as<double>(), g->nz.as<double>(), g->w.as<double>(), g->n, g->perm.as<int32_t>()};
 }
 
 template <class T>
@@ -590,6 +591,7 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
         throw Error(BIE_ENODEVICE, "no CUDA device available (libbie_b200 has no CPU fallback)");
     }
     if (device < 0 || device >= ndev) throw Error(BIE_EINVAL, "device ordinal out of range");
+    if (n >= (int64_t)1 << 31) throw Error(BIE_EUNSUPPORTED, "at most 2^31 - 1 nodes per geometry");
     DeviceGuard dg(device);
     std::unique_ptr<bie_geom> g(new bie_geom());
     g->device = device;
@@ -615,6 +617,37 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
     }
     upload(g->w, w, n, s);
     upload(g->diag, diag, n, s);
+    // Morton (Z-order) permutation of the nodes: 21-bit quantised coordinates, bits interleaved
+    {
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int64_t i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) {
+                lo[c] = std::min(lo[c], pts[3 * i + c]);
+                hi[c] = std::max(hi[c], pts[3 * i + c]);
+            }
+        const double ext = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+        auto spread = [](uint64_t v) {  // 21 bits -> every third bit of 63
+            v &= 0x1FFFFFull;
+            v = (v | v << 32) & 0x1F00000000FFFFull;
+            v = (v | v << 16) & 0x1F0000FF0000FFull;
+            v = (v | v << 8) & 0x100F00F00F00F00Full;
+            v = (v | v << 4) & 0x10C30C30C30C30C3ull;
+            v = (v | v << 2) & 0x1249249249249249ull;
+            return v;
+        };
+        std::vector<std::pair<uint64_t, int32_t>> key((size_t)n);
+        for (int64_t i = 0; i < n; ++i) {
+            uint64_t q[3];
+            for (int c = 0; c < 3; ++c)
+                q[c] = (uint64_t)std::min(2097151.0, std::floor((pts[3 * i + c] - lo[c]) / ext * 2097151.0));
+            key[i] = {spread(q[0]) | spread(q[1]) << 1 | spread(q[2]) << 2, (int32_t)i};
+        }
+        std::stable_sort(key.begin(), key.end(), [](auto& a, auto& b) { return a.first < b.first; });
+        std::vector<int32_t> perm((size_t)n);
+        for (int64_t i = 0; i < n; ++i) perm[i] = key[i].second;
+        upload(g->perm, perm.data(), n, s);
+        BIE_CK(cudaStreamSynchronize(s));
+    }
     g->errflag.ensure(sizeof(int));
     BIE_CK(cudaMemsetAsync(g->errflag.p, 0, sizeof(int), s));
     for (int64_t i = 0; i < n; ++i) col3[i] = diag[i] != 0.0 ? 1.0 / diag[i] : 1.0;
@@ -635,7 +668,7 @@ void geom_destroy(bie_geom* g) {
     {
         DeviceGuard dg(g->device);
         if (g->stream) cudaStreamSynchronize(g->stream);
-        bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->rowptr,
+        bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->perm, &g->rowptr,
                            &g->col, &g->val, &g->part, &g->small, &g->bpack, &g->errflag, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
                            &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
