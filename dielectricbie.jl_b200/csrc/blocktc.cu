@@ -10,16 +10,25 @@
 // mul!(Y, ::BatchedDielectricOperator, X) (src/solver/multi_rhs.jl:103-130).
 //
 // Split-BF16 three-term product: with G = Gh + Gl and Q = Qh + Ql (bf16 hi/lo),
-// G Q ~= Gh Qh + Gh Ql + Gl Qh (the dropped Gl Ql term is ~2^-16 relative),
-// accumulated in FP32 in tensor memory; each source split writes an FP64 partial.
+// G Q ~= Gh Qh + Gh Ql + Gl Qh (the dropped Gl Ql term is ~2^-16 relative).
+// The tensor cores accumulate FP32 in tensor memory over FP = 4 chunks (256
+// sources) into one of two alternating accumulators; the generator threads add
+// each finished period into an FP32 running sum also kept in tensor memory. The
+// tensor-core accumulation error grows with the number of accumulation steps;
+// restarting it every period bounds it by that of 256 sources, and the running
+// sum of the periods (round-to-nearest additions) adds a random-walk error of a
+// few units in the last place. Each source split writes the sum as an FP64 partial.
 //
-// CTA = 320 threads: warps 0-7 generate the 128 x 64 kernel tile of a source
-// chunk (two threads per target row, each writing 32 of the row's 64 K-major
-// bf16 values into the 128-byte swizzled layout the UMMA descriptors read) and
-// run the epilogue; warp 8 issues the MMAs (one thread); warp 9 streams the
-// pre-swizzled Q tiles with bulk copies. Box faces are axis-aligned, so a warp
-// whose 32 rows share a normal axis computes n.(x - y) as the signed axis
-// difference and folds the sign into its epilogue.
+// CTA = 128 NQ + 64 threads: warps 0 .. 4 NQ - 1 generate the 128 x 64 kernel tile
+// of a source chunk (NQ threads per target row, each writing 64 / NQ of the row's
+// K-major bf16 values into the 128-byte swizzled layout the UMMA descriptors
+// read), fold the accumulators and run the epilogue; the next warp issues the MMAs
+// (one thread); the last warp streams the pre-swizzled Q tiles with bulk copies
+// into a ring and stages the source coordinates SC - 1 chunks ahead. Up to 64
+// columns run two CTAs per SM (NQ = 2), so that one CTA's pipeline bubbles are
+// filled by the other; wider tiles run one CTA per SM with NQ = 4. Box faces are
+// axis-aligned, so a warp whose 32 rows share a normal axis computes n.(x - y) as
+// the signed axis difference and folds the sign into its epilogue.
 // Every mbarrier wait is bounded: on expiry the CTA records an error code and
 // returns after releasing its tensor memory.
 #include <cuda_bf16.h>
@@ -35,10 +44,23 @@ namespace tc {
 
 constexpr int M = 128;      // targets per tile (MMA M)
 constexpr int KC = 64;      // sources per chunk = one 128-byte bf16 row
-constexpr int S = 2;        // pipeline stages
-constexpr int NGEN = 256;      // generator threads: 2 per tile row (two halves of a chunk)
-constexpr int NTHREADS = NGEN + 64;
-constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr int SAMAX = 4;    // A (kernel tile) ring stages at most (Params::sa)
+constexpr int SBMAX = 4;    // B (Q tile) ring stages at most (Params::sb)
+constexpr int SC = 4;       // source-coordinate ring stages (staged SC - 1 chunks ahead)
+// NQ = generator threads per tile row (each 64 / NQ sources of a chunk): 2 for the
+// two-CTAs-per-SM shape (320 threads, <= 96 registers), 4 for the one-CTA shape
+// (576 threads, <= 112 registers).
+template <int NQ> __host__ __device__ constexpr int ngen() { return M * NQ; }
+template <int NQ> __host__ __device__ constexpr int nthreads() { return M * NQ + 64; }
+// Tensor-memory columns of a CTA: two accumulators and the running sum, npad
+// columns each, rounded up to the power-of-two allocation unit.
+__host__ __device__ inline uint32_t tmem_cols(int npad) {
+    uint32_t c = 32;
+    while (c < 3u * (uint32_t)npad) c <<= 1;
+    return c;
+}
+constexpr int FP = 4;          // chunks accumulated in FP32 tensor memory before a compensated fold
+constexpr uint32_t kWaitLimit = 1u << 26;  // wait attempts before a CTA gives up (seconds)
 constexpr int kErrTimeout = 1;
 
 struct Params {
@@ -48,6 +70,7 @@ struct Params {
     int keff;              // columns stored (<= npad)
     int64_t nchunks;
     int64_t cps;           // chunks per split
+    int sa, sb;            // A and B ring stages (2 .. SAMAX, 2 .. SBMAX)
     double* part;          // [nsplit][n][ldp]
     int ldp, c0;
     int* err;
@@ -75,11 +98,16 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ bool flag_set(volatile int* f) {
+    int v;
+    asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32((const void*)f)) : "memory");
+    return v != 0;
+}
 // Bounded wait; returns false (and flags the CTA) when the limit expires.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
     for (uint32_t it = 0; it < kWaitLimit; ++it) {
         if (mbar_try(b, parity)) return true;
-        if (*abort_flag) return false;
+        if (flag_set(abort_flag)) return false;
     }
     *abort_flag = 1;
     return false;
@@ -92,17 +120,18 @@ __device__ __forceinline__ bool mbar_wait_raw(uint64_t* b, uint32_t parity) {
     return false;
 }
 
-// OR-reduction of a predicate over the 256 generator threads (named barrier 1):
+// OR-reduction of a predicate over the NG generator threads (named barrier 1):
 // also orders their shared-memory accesses like bar.sync.
+template <int NG>
 __device__ __forceinline__ bool gen_any(bool v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, 1, 256, q;\n\t"
+        "bar.red.or.pred p, 1, %2, q;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)v)
+        : "r"((uint32_t)v), "n"(NG)
         : "memory");
     return r != 0;
 }
@@ -145,6 +174,16 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+// Issues a 32-lane x 16-column tensor-memory load; the registers are valid after tmem_wait_ld().
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];
     asm volatile(
@@ -162,6 +201,18 @@ __device__ __forceinline__ float rsqrt_mufu(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+        "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+        "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem) {
@@ -184,34 +235,34 @@ __device__ __forceinline__ void split_pieces(float a, float b, uint32_t* out) {
     }
 }
 
-// One thread's half row of a chunk's kernel tile: 32 sources (groups gq0..gq0+3),
-// processed 16 at a time. AX = 0/1/2: the rows of this warp have normal +-e_AX
-// (sign applied in the epilogue); AX = 3: general normal.
-template <int AX, int NP>
-__device__ __forceinline__ void gen_half_row(const float* __restrict__ cs, float xi, float yi, float zi, float n0,
+// One thread's share of a row of a chunk's kernel tile: 64 / NQ sources (8-source
+// groups gq0 .. gq0 + 8 / NQ - 1), processed 16 at a time. AXIS: the rows of this
+// warp have normal +-e_a for one axis a (sign applied in the epilogue); ca holds the
+// source coordinates along a and cb, cc the other two, ta, tb, tc the target's in
+// the same order, so one code path serves the three axes. !AXIS: general normal
+// (n0, n1, n2), with (ca, cb, cc) = (x, y, z).
+template <bool AXIS, int NP, int NQ>
+__device__ __forceinline__ void gen_row_part(const float* __restrict__ ca, const float* __restrict__ cb,
+                                             const float* __restrict__ cc, float ta, float tb, float tc, float n0,
                                              float n1, float n2, int gq0, bool self, int64_t j0, int64_t i,
                                              uint8_t* Astage, uint32_t a_bytes, uint32_t row_off, uint32_t rsw) {
 #pragma unroll 1
-    for (int gq = gq0; gq < gq0 + 4; gq += 2) {
+    for (int gq = gq0; gq < gq0 + 8 / NQ; gq += 2) {
         float v[16];
 #pragma unroll
         for (int e4 = 0; e4 < 4; ++e4) {
             const int b = gq * 8 + e4 * 4;
-            const float4 X4 = *reinterpret_cast<const float4*>(cs + b);
-            const float4 Y4 = *reinterpret_cast<const float4*>(cs + KC + b);
-            const float4 Z4 = *reinterpret_cast<const float4*>(cs + 2 * KC + b);
-            const float sx[4] = {X4.x, X4.y, X4.z, X4.w}, sy[4] = {Y4.x, Y4.y, Y4.z, Y4.w},
-                        sz[4] = {Z4.x, Z4.y, Z4.z, Z4.w};
+            const float4 A4 = *reinterpret_cast<const float4*>(ca + b);
+            const float4 B4 = *reinterpret_cast<const float4*>(cb + b);
+            const float4 C4 = *reinterpret_cast<const float4*>(cc + b);
+            const float sa[4] = {A4.x, A4.y, A4.z, A4.w}, sb[4] = {B4.x, B4.y, B4.z, B4.w},
+                        sc[4] = {C4.x, C4.y, C4.z, C4.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const float dx = xi - sx[e], dy = yi - sy[e], dz = zi - sz[e];
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float da = ta - sa[e], db = tb - sb[e], dc = tc - sc[e];
+                const float r2 = fmaf(da, da, fmaf(db, db, dc * dc));
                 const float ri = rsqrt_mufu(r2);
-                float dn;
-                if (AX == 0) dn = dx;
-                else if (AX == 1) dn = dy;
-                else if (AX == 2) dn = dz;
-                else dn = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
+                const float dn = AXIS ? da : fmaf(n0, da, fmaf(n1, db, n2 * dc));
                 v[e4 * 4 + e] = (dn * ri) * (ri * ri);
             }
         }
@@ -233,22 +284,28 @@ __device__ __forceinline__ void gen_half_row(const float* __restrict__ cs, float
     }
 }
 
-template <int NP>
-__global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
+template <int NP, int NQ>
+__global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
+    constexpr int NGEN = ngen<NQ>();
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // carve-up aligned to 1024 bytes in the shared window (128-byte swizzle atoms)
     uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int npad = P.npad;
-    const uint32_t a_bytes = M * 128;          // one term of the A tile (16 KB)
-    const uint32_t b_bytes = (uint32_t)npad * 128;  // one term of the B tile
-    uint8_t* A = base;                               // [S][NP][a_bytes]
-    uint8_t* B = A + S * NP * a_bytes;               // [S][NP][b_bytes]
-    float* crd = (float*)(B + S * NP * b_bytes);     // [S][3][KC] source coordinates (SoA, FP32 relative)
-    uint64_t* full_a = (uint64_t*)(crd + S * 3 * KC);
-    uint64_t* full_b = full_a + S;
-    uint64_t* empty = full_b + S;
-    uint64_t* crd_full = empty + S;
-    uint64_t* acc_done = crd_full + S;
+    const uint32_t a_bytes = M * 128;          // one piece of the A tile (16 KB)
+    const uint32_t b_bytes = (uint32_t)npad * 128;  // one piece of the B tile
+    const int SA = P.sa, SB = P.sb;
+    uint8_t* A = base;                               // [SA][NP][a_bytes]
+    uint8_t* B = A + SA * NP * a_bytes;              // [SB][NP][b_bytes]
+    float* crd = (float*)(B + SB * NP * b_bytes);    // [SC][3][KC] source coordinates (SoA, FP32 relative)
+    uint64_t* full_a = (uint64_t*)(crd + SC * 3 * KC);
+    uint64_t* empty_a = full_a + SAMAX;  // [SAMAX] A stage consumed (MMA commit)
+    uint64_t* full_b = empty_a + SAMAX;  // [SBMAX] Q tile landed (bulk copy)
+    uint64_t* empty_b = full_b + SBMAX;  // [SBMAX] Q tile consumed (MMA commit)
+    uint64_t* crd_full = empty_b + SBMAX;  // [SC] coordinates staged (producer warp)
+    uint64_t* crd_empty = crd_full + SC; // [SC] coordinates consumed (generators)
+    uint64_t* acc_full = crd_empty + SC; // [2] accumulation period finished (MMA commit)
+    uint64_t* acc_empty = acc_full + 2;  // [2] accumulator folded (generators)
+    uint64_t* acc_done = acc_empty + 2;
     uint32_t* tmem_slot = (uint32_t*)(acc_done + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
@@ -258,14 +315,26 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     const int64_t ch0 = (int64_t)blockIdx.y * P.cps;
     const int64_t ch1 = min(P.nchunks, ch0 + P.cps);
     const int nch = ch1 > ch0 ? (int)(ch1 - ch0) : 0;
-    const uint32_t tcols = npad <= 32 ? 32 : (npad <= 64 ? 64 : (npad <= 128 ? 128 : 256));
+    // tensor memory: two FP32 accumulators (alternating periods) and the running
+    // sum, npad columns each
+    const uint32_t tcols = tmem_cols(npad);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
+        for (int s = 0; s < SAMAX; ++s) {
             mbar_init(&full_a[s], NGEN);
+            mbar_init(&empty_a[s], 1);
+        }
+        for (int s = 0; s < SBMAX; ++s) {
             mbar_init(&full_b[s], 1);
-            mbar_init(&empty[s], 1);
+            mbar_init(&empty_b[s], 1);
+        }
+        for (int s = 0; s < SC; ++s) {
             mbar_init(&crd_full[s], 32);
+            mbar_init(&crd_empty[s], NGEN);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], NGEN);
         }
         mbar_init(acc_done, 1);
         *abort_flag = 0;
@@ -281,6 +350,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    const uint32_t t_sum = tmem + 2u * (uint32_t)npad;
 
     // tile origin: coordinates are rounded to FP32 relative to it
     const int64_t io = P.g.perm[min(i0, n - 1)];
@@ -289,7 +359,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
     if (warp < NGEN / 32) {
         // ------------------------- generators -------------------------------
         const int r = threadIdx.x & (M - 1);  // tile row
-        const int half = threadIdx.x / M;     // which 32 sources of each chunk
+        const int qt = threadIdx.x / M;       // which 64 / NQ sources of each chunk (warp-uniform)
         const bool valid = i0 + r < n;
         const int64_t i = valid ? (int64_t)P.g.perm[i0 + r] : n;  // original index of the target
         float xi, yi, zi, n0, n1, n2;
@@ -311,47 +381,91 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
         const int cmax = __reduce_max_sync(full, valid ? code : -1);
         const int ax = (cmin == cmax && cmin < 3) ? cmin : 3;
         if (ax == 3) sgn = 1.f;
+        // axis path: the normal axis first, then the other two (coordinate-array
+        // offsets in the staged chunk and the target's coordinates in that order)
+        const int a1 = ax < 3 ? ax : 0, a2 = a1 == 2 ? 0 : a1 + 1, a3 = a2 == 2 ? 0 : a2 + 1;
+        const int oa = a1 * KC, ob = a2 * KC, oc = a3 * KC;
+        const float tcrd[3] = {xi, yi, zi};
+        const float ta = a1 == 0 ? tcrd[0] : (a1 == 1 ? tcrd[1] : tcrd[2]);
+        const float tb = a2 == 0 ? tcrd[0] : (a2 == 1 ? tcrd[1] : tcrd[2]);
+        const float tc = a3 == 0 ? tcrd[0] : (a3 == 1 ? tcrd[1] : tcrd[2]);
         const uint32_t row_off = (uint32_t)r * 128u;
         const uint32_t rsw = (uint32_t)(r & 7);
-        for (int lc = 0; lc < nch; ++lc) {
-            const int s = lc % S;
-            const uint32_t u = (uint32_t)(lc / S);
-            const int64_t j0 = (ch0 + lc) * KC;
-            // coordinates staged (and stage s released by the MMAs of chunk lc - S)
-            if (!mbar_wait(&crd_full[s], u & 1, abort_flag)) break;
-            uint8_t* As = A + s * NP * a_bytes;
-            const float* cs = crd + s * 3 * KC;
-            const bool self = (i >= j0) && (i < j0 + KC);  // this chunk holds the target's own node
-            const int gq0 = half * 4;
-            switch (ax) {
-                case 0: gen_half_row<0, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
-                case 1: gen_half_row<1, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
-                case 2: gen_half_row<2, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
-                default: gen_half_row<3, NP>(cs, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As, a_bytes, row_off, rsw); break;
+        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+
+        // Add the FP32 accumulator of period p into the running sum; the warp
+        // decides as a whole.
+        auto fold = [&](int p) -> bool {
+            const int b = p & 1;
+            bool ok = mbar_wait(&acc_full[b], (uint32_t)(p >> 1) & 1u, abort_flag);
+            if (!__all_sync(full, ok)) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int c = qt * 16; c < npad; c += 16 * NQ) {
+                uint32_t a[16], h[16];
+                tmem_ld16_async(tmem + lane_base + (uint32_t)(b * npad + c), a);
+                if (p == 0) {
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) h[q] = a[q];
+                } else {
+                    tmem_ld16_async(t_sum + lane_base + (uint32_t)c, h);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) h[q] = __float_as_uint(__uint_as_float(h[q]) + __uint_as_float(a[q]));
+                }
+                tmem_st16(t_sum + lane_base + (uint32_t)c, reinterpret_cast<const float*>(h));
             }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&acc_empty[b]);
+            return true;
+        };
+
+        bool ok = true;
+        for (int lc = 0; lc < nch && ok; ++lc) {
+            const int s = lc % SA, sc = lc % SC;
+            const int64_t j0 = (ch0 + lc) * KC;
+            // coordinates staged; A stage s released by the MMAs of chunk lc - S
+            if (!mbar_wait(&crd_full[sc], (uint32_t)(lc / SC) & 1u, abort_flag)) { ok = false; break; }
+            if (lc >= SA && !mbar_wait(&empty_a[s], (uint32_t)(lc / SA - 1) & 1u, abort_flag)) { ok = false; break; }
+            uint8_t* As = A + s * NP * a_bytes;
+            const float* cs = crd + sc * 3 * KC;
+            const bool self = (i >= j0) && (i < j0 + KC);  // this chunk holds the target's own node
+            const int gq0 = qt * (8 / NQ);
+            if (ax < 3)
+                gen_row_part<true, NP, NQ>(cs + oa, cs + ob, cs + oc, ta, tb, tc, n0, n1, n2, gq0, self, j0, i, As,
+                                           a_bytes, row_off, rsw);
+            else
+                gen_row_part<false, NP, NQ>(cs, cs + KC, cs + 2 * KC, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As,
+                                            a_bytes, row_off, rsw);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&full_a[s]);
+            mbar_arrive(&crd_empty[sc]);
+            // end of period p: fold period p - 1 (its MMAs finished while p was generated)
+            if (lc % FP == FP - 1 || lc == nch - 1) {
+                const int p = lc / FP;
+                if (p >= 1) ok = fold(p - 1);
+            }
         }
         // ------------------------- epilogue ---------------------------------
-        bool ok = !*abort_flag;
-        if (nch > 0 && ok) ok = mbar_wait(acc_done, 0, abort_flag);
-        ok = !gen_any(!ok);  // every generator warp takes the same branch
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        ok = ok && !*abort_flag;
+        if (nch > 0 && ok) ok = fold((nch - 1) / FP);
+        ok = !gen_any<NGEN>(!ok);  // every generator warp takes the same branch
         if (ok) {
-            const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             double* out = P.part + ((int64_t)blockIdx.y * n + i) * P.ldp + P.c0;
-            for (int c = half * 16; c < npad; c += 32) {
-                float v[16];
+            for (int c = qt * 16; c < npad; c += 16 * NQ) {
+                float h[16];
                 if (nch > 0) {
-                    tmem_ld16(tmem + lane_base + (uint32_t)c, v);
+                    tmem_ld16(t_sum + lane_base + (uint32_t)c, h);
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) v[q] = 0.f;
+                    for (int q = 0; q < 16; ++q) h[q] = 0.f;
                 }
                 if (valid) {
 #pragma unroll
                     for (int q = 0; q < 16; ++q)
-                        if (c + q < P.keff) out[c + q] = (double)(sgn * v[q]);
+                        if (c + q < P.keff) out[c + q] = (double)sgn * (double)h[q];
                 }
             }
         }
@@ -360,27 +474,35 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
         if (lane == 0) {
             const uint32_t idesc = idesc_bf16(npad);
             for (int lc = 0; lc < nch; ++lc) {
-                const int s = lc % S;
-                const uint32_t u = (uint32_t)(lc / S);
-                if (!mbar_wait(&full_a[s], u & 1, abort_flag)) break;
-                if (!mbar_wait(&full_b[s], u & 1, abort_flag)) break;
+                const int s = lc % SA, sb = lc % SB;
+                const int p = lc / FP, b = p & 1;
+                const bool pfirst = (lc % FP) == 0;
+                if (!mbar_wait(&full_a[s], (uint32_t)(lc / SA) & 1u, abort_flag)) break;
+                if (!mbar_wait(&full_b[sb], (uint32_t)(lc / SB) & 1u, abort_flag)) break;
+                // accumulator b is reused from period p - 2 once the generators folded it
+                if (pfirst && p >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)((p - 2) >> 1) & 1u, abort_flag)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t a0 = smem_u32(A + s * NP * a_bytes), b0 = smem_u32(B + s * NP * b_bytes);
+                // descriptors of the stage; the start-address field (bits 0-13, address >> 4)
+                // is advanced in place: every address stays below 256 KB
+                const uint64_t da = sw128_desc(smem_u32(A + s * NP * a_bytes));
+                const uint64_t db = sw128_desc(smem_u32(B + sb * NP * b_bytes));
+                const uint32_t dacc = tmem + (uint32_t)(b * npad);
                 // products of pieces whose orders sum to at most NP - 1
 #pragma unroll
                 for (int kk = 0; kk < KC / 16; ++kk) {
-                    const uint32_t ko = (uint32_t)kk * 32u;
-                    bool first = (lc == 0 && kk == 0);
+                    bool first = pfirst && kk == 0;
 #pragma unroll
                     for (int pa = 0; pa < NP; ++pa)
 #pragma unroll
                         for (int pb = 0; pb + pa < NP; ++pb) {
-                            mma_bf16(tmem, sw128_desc(a0 + pa * a_bytes + ko), sw128_desc(b0 + pb * b_bytes + ko), idesc,
-                                     first ? 0u : 1u);
+                            mma_bf16(dacc, da + (uint64_t)((pa * a_bytes + kk * 32) >> 4),
+                                     db + (uint64_t)((pb * b_bytes + kk * 32) >> 4), idesc, first ? 0u : 1u);
                             first = false;
                         }
                 }
-                mma_commit(&empty[s]);
+                mma_commit(&empty_a[s]);
+                mma_commit(&empty_b[sb]);
+                if (lc % FP == FP - 1 || lc == nch - 1) mma_commit(&acc_full[b]);
             }
             mma_commit(acc_done);
             // on abort, drain this thread's MMAs before the CTA releases tensor memory
@@ -389,35 +511,55 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_dt_tc(Params P) {
         __syncwarp();
     } else {
         // ------------- Q-tile and source-coordinate producer -----------------
+        // Runs SB - 1 chunks ahead on the Q tiles and SC - 1 chunks ahead on the
+        // coordinates; each slot is refilled once its consumer of SB (SC) chunks
+        // earlier has finished.
         const uint32_t bytes = NP * b_bytes;
         int issued = 0;
-        for (int lc = 0; lc < nch; ++lc) {
-            const int s = lc % S;
-            const uint32_t u = (uint32_t)(lc / S);
-            if (lc >= S && !mbar_wait(&empty[s], (u - 1) & 1, abort_flag)) break;
+        auto stage_b = [&](int c) -> bool {
+            const int sb = c % SB;
+            if (c >= SB && !mbar_wait(&empty_b[sb], (uint32_t)(c / SB - 1) & 1u, abort_flag)) return false;
             if (lane == 0) {
-                mbar_arrive_tx(&full_b[s], bytes);
-                bulk_g2s(B + s * NP * b_bytes, P.bpack + (size_t)(ch0 + lc) * bytes, bytes, &full_b[s]);
-                issued = lc + 1;
+                mbar_arrive_tx(&full_b[sb], bytes);
+                bulk_g2s(B + sb * NP * b_bytes, P.bpack + (size_t)(ch0 + c) * bytes, bytes, &full_b[sb]);
+                issued = c + 1;
             }
-            // source coordinates of the chunk, FP32 relative to the tile origin
-            float* cs = crd + s * 3 * KC;
-            const int64_t j0 = (ch0 + lc) * KC;
+            return true;
+        };
+        // coordinates of chunk c, FP32 relative to the tile origin; the global
+        // loads are issued before the wait for the slot
+        auto stage_crd = [&](int c) -> bool {
+            const int64_t j0 = (ch0 + c) * KC;
+            float x[KC / 32], y[KC / 32], z[KC / 32];
+#pragma unroll
+            for (int h = 0; h < KC / 32; ++h) {
+                const int64_t j = j0 + lane + 32 * h;
+                x[h] = y[h] = z[h] = 1.0e18f;  // padded source: G underflows to 0
+                if (j < n) {
+                    x[h] = (float)(P.g.x[j] - ox); y[h] = (float)(P.g.y[j] - oy); z[h] = (float)(P.g.z[j] - oz);
+                }
+            }
+            const int sc = c % SC;
+            if (c >= SC && !mbar_wait(&crd_empty[sc], (uint32_t)(c / SC - 1) & 1u, abort_flag)) return false;
+            float* cs = crd + sc * 3 * KC;
 #pragma unroll
             for (int h = 0; h < KC / 32; ++h) {
                 const int t = lane + 32 * h;
-                const int64_t j = j0 + t;
-                float x = 1.0e18f, y = 1.0e18f, z = 1.0e18f;  // padded source: G underflows to 0
-                if (j < n) {
-                    x = (float)(P.g.x[j] - ox); y = (float)(P.g.y[j] - oy); z = (float)(P.g.z[j] - oz);
-                }
-                cs[t] = x; cs[KC + t] = y; cs[2 * KC + t] = z;
+                cs[t] = x[h]; cs[KC + t] = y[h]; cs[2 * KC + t] = z[h];
             }
-            mbar_arrive(&crd_full[s]);
+            mbar_arrive(&crd_full[sc]);
+            return true;
+        };
+        bool ok = true;
+        for (int c = 0; c < SC - 1 && c < nch && ok; ++c) ok = stage_crd(c);
+        for (int c = 0; c < SB - 1 && c < nch && ok; ++c) ok = stage_b(c);
+        for (int lc = 0; lc < nch && ok; ++lc) {
+            if (lc + SB - 1 < nch) ok = stage_b(lc + SB - 1);
+            if (ok && lc + SC - 1 < nch) ok = stage_crd(lc + SC - 1);
         }
-        // on abort, wait for the copies still in flight (at most one per stage)
+        // on abort, wait for the copies still in flight (at most one per slot)
         if (lane == 0 && *abort_flag)
-            for (int lc = issued > S ? issued - S : 0; lc < issued; ++lc) mbar_wait_raw(&full_b[lc % S], (lc / S) & 1);
+            for (int c = issued > SB ? issued - SB : 0; c < issued; ++c) mbar_wait_raw(&full_b[c % SB], (c / SB) & 1);
         __syncwarp();
     }
 
@@ -461,11 +603,62 @@ __global__ void k_pack_q(GeomDev g, const double* __restrict__ X, int ldx, int c
         *reinterpret_cast<uint4*>(base + p * tile + off) = make_uint4(w[0][p], w[1][p], w[2][p], w[3][p]);
 }
 
-size_t smem_bytes(int npad, int np) {
-    size_t a = (size_t)S * np * M * 128, b = (size_t)S * np * npad * 128;
-    size_t c = (size_t)S * 3 * KC * sizeof(float);
-    size_t bars = (4 * S + 1) * sizeof(uint64_t) + 16;
+size_t smem_bytes(int npad, int np, int sa, int sb) {
+    size_t a = (size_t)sa * np * M * 128, b = (size_t)sb * np * npad * 128;
+    size_t c = (size_t)SC * 3 * KC * sizeof(float);
+    size_t bars = (2 * SAMAX + 2 * SBMAX + 2 * SC + 5) * sizeof(uint64_t) + 16;
     return 1024 + a + b + c + bars;
+}
+
+// Ring depths for one CTA per SM: the deepest A ring (<= SAMAX) that fits with a
+// 2-slot B ring (the kernel-tile generators run SA - 1 chunks ahead of the MMAs),
+// then the deepest B ring that still fits.
+void ring_stages(int npad, int np, int* sa, int* sb) {
+    const size_t cap = 227 * 1024;
+    int a = SAMAX;
+    while (a > 2 && smem_bytes(npad, np, a, 2) > cap) --a;
+    int b = SBMAX;
+    while (b > 2 && smem_bytes(npad, np, a, b) > cap) --b;
+    *sa = a;
+    *sb = b;
+}
+
+// Launch shape for npad columns and np pieces: two CTAs per SM (NQ = 2, A ring of
+// two) when their tensor memory (3 npad columns each, allocated as a power of two)
+// and shared memory fit, else
+// one CTA per SM (NQ = 4) with the deepest rings that fit.
+struct Shape {
+    int ctas, nq, sa, sb;
+    size_t smem;
+};
+
+Shape shape(int npad, int np) {
+    const size_t half_sm = 113 * 1024;  // 228 KB per SM, 1 KB reserved per CTA
+    Shape sh;
+    if (tmem_cols(npad) <= 256 && smem_bytes(npad, np, 2, 2) <= half_sm) {
+        sh.ctas = 2;
+        sh.nq = 2;
+        sh.sa = 2;
+        sh.sb = 2;
+        while (sh.sb < SBMAX && smem_bytes(npad, np, 2, sh.sb + 1) <= half_sm) ++sh.sb;
+    } else {
+        sh.ctas = 1;
+        sh.nq = 4;
+        ring_stages(npad, np, &sh.sa, &sh.sb);
+    }
+    sh.smem = smem_bytes(npad, np, sh.sa, sh.sb);
+    return sh;
+}
+
+template <int NP, int NQ>
+void launch_k(const Params& P, dim3 grid, size_t sm, cudaStream_t s) {
+    static size_t configured = 0;
+    if (sm > configured) {
+        BIE_CK(cudaFuncSetAttribute(k_dt_tc<NP, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        configured = sm;
+    }
+    k_dt_tc<NP, NQ><<<grid, nthreads<NQ>(), sm, s>>>(P);
+    BIE_CK(cudaGetLastError());
 }
 
 template <int NP>
@@ -483,26 +676,25 @@ void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const
     P.keff = kc;
     P.nchunks = nchunks;
     P.cps = cps;
+    const Shape sh = shape(npad, NP);
+    P.sa = sh.sa;
+    P.sb = sh.sb;
     P.part = part;
     P.ldp = ldp;
     P.c0 = c0;
     P.err = err;
-    const size_t sm = smem_bytes(npad, NP);
-    static size_t configured = 0;
-    if (sm > configured) {
-        BIE_CK(cudaFuncSetAttribute(k_dt_tc<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        configured = sm;
-    }
     dim3 grid((unsigned)((g.n + M - 1) / M), (unsigned)nsplit);
-    k_dt_tc<NP><<<grid, NTHREADS, sm, s>>>(P);
-    BIE_CK(cudaGetLastError());
+    if (sh.nq == 2)
+        launch_k<NP, 2>(P, grid, sh.smem, s);
+    else
+        launch_k<NP, 4>(P, grid, sh.smem, s);
 }
 
 }  // namespace tc
 
 int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
 
-// Runs K3 for columns [c0, c0 + kc) (kc <= 256) of X into part[s][i][c0 + c],
+// Runs K3 for columns [c0, c0 + kc) (kc <= 128) of X into part[s][i][c0 + c],
 // with the kernel and right-hand sides split into `pieces` (2: three products,
 // 3: six products) bf16 pieces.
 void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
@@ -518,9 +710,6 @@ size_t block_tc_pack_bytes(int64_t n, int kc, int pieces) {
     return (size_t)nchunks * pieces * tc_npad(kc) * 128;
 }
 
-int block_tc_ctas_per_sm(int kc, int pieces) {
-    const size_t sm = tc::smem_bytes(tc_npad(kc), pieces);
-    return std::max(1, (int)((227 * 1024) / (sm + 1024)));
-}
+int block_tc_ctas_per_sm(int kc, int pieces) { return tc::shape(tc_npad(kc), pieces).ctas; }
 
 }  // namespace bie

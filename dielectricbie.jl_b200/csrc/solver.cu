@@ -260,15 +260,28 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
     return sp;
 }
 
-// K3 launch plan: enough source splits for >= 2 waves of CTAs, and at most 256
-// chunks (16384 sources) accumulated in FP32 tensor memory per FP64 partial.
+// K3 launch plan: the number of source splits ns (<= 16, and at most 1024 chunks
+// per split) that minimises the time of the wave-quantised grid, which is
+// proportional to ceil(tiles ns / slots) / ns; ties go to fewer splits (each
+// split adds an FP64 partial for the combine to read).
 Split tc_split(const bie_geom* g, int kc, int pieces) {
     const int64_t tiles = (g->n + kTcTileM - 1) / kTcTileM;
     const int64_t chunks = (g->n + kTcChunk - 1) / kTcChunk;
     const int64_t slots = (int64_t)g->sms * block_tc_ctas_per_sm(kc, pieces);
-    int64_t ns = std::max<int64_t>(1, (2 * slots + tiles - 1) / tiles);
-    ns = std::max<int64_t>(ns, (chunks + 255) / 256);
-    ns = std::min<int64_t>(ns, chunks);
+    const int64_t ns_min = std::min<int64_t>(chunks, std::max<int64_t>(1, (chunks + 1023) / 1024));
+    const int64_t ns_max = std::min<int64_t>(chunks, std::max<int64_t>(ns_min, 16));
+    int64_t ns = ns_min;
+    double best = 1e300;
+    for (int64_t t = ns_min; t <= ns_max; ++t) {
+        const int64_t cps_t = (chunks + t - 1) / t;
+        const int64_t nt = (chunks + cps_t - 1) / cps_t;  // splits actually launched
+        const double waves = (double)((tiles * nt + slots - 1) / slots);
+        const double cost = waves * (double)cps_t * (1.0 + 0.002 * (double)nt);
+        if (cost < best - 1e-9) {
+            best = cost;
+            ns = t;
+        }
+    }
     int64_t cps = (chunks + ns - 1) / ns;
     ns = (chunks + cps - 1) / cps;
     return Split{(int)ns, cps};
@@ -276,11 +289,11 @@ Split tc_split(const bie_geom* g, int kc, int pieces) {
 
 Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, int pieces, cudaStream_t s) {
     GeomDev gd = gdev(g);
-    Split sp = tc_split(g, std::min(k, 256), pieces);
+    Split sp = tc_split(g, std::min(k, 128), pieces);
     g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
-    g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 256), pieces));
-    for (int c0 = 0; c0 < k; c0 += 256) {
-        int kc = std::min(256, k - c0);
+    g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 128), pieces));
+    for (int c0 = 0; c0 < k; c0 += 128) {
+        int kc = std::min(128, k - c0);
         const double npairs = (double)g->n * (g->n - 1);
         Prof pf(g, BIE_KERNEL_DIRECT_TC, s, 2, npairs, npairs * tc_npad(kc));
         launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, g->bpack.as<uint8_t>(),

@@ -148,7 +148,7 @@ def test_potential_and_energy(bie, orc, cfg1, rng):
         assert abs(W[c] - ref_c) <= 1e-13 * abs(ref_c)
 
 
-@pytest.mark.parametrize("k", [16, 20, 64])
+@pytest.mark.parametrize("k", [16, 20, 64, 144])
 def test_matvec_bf16x3_tensor_core(bie, cfg1, rng, k):
     """K3 (tcgen05 split-BF16 three-term contraction) vs the FP64 operator: the dropped
     lo*lo term and FP32 accumulation bound the error near 1e-5 relative."""
@@ -187,6 +187,21 @@ def test_matvec_bf16x6_tensor_core(bie, cfg1, rng):
     Y3 = op.mul(X, precision="bf16x3")
     assert rel(Y6, Y64) < 5e-7  # FP32-level: the FP32 kernel generation bounds it
     assert rel(Y6, Y64) < rel(Y3, Y64)
+
+
+def test_tensor_core_accumulation_does_not_grow_with_n(bie, rng):
+    """42048 nodes (657 source chunks per target tile): the FP32 tensor-memory sums are
+    folded into a two-sum pair every 256 sources, so BF16x3 stays at the FP32-kernel
+    level instead of growing with the number of sources."""
+    itf = bie.single_dielectric_box3d(1.5, 1.0, 0.8, 6, 0.08, 4.0, 1.0)
+    assert itf.n == 42048
+    op = bie.lhs_dielectric_box3d(itf)
+    X = rng.standard_normal((itf.n, 16))
+    Y64 = op.mul(X)
+    Y32 = op.mul(X, precision="fp32")
+    Y3 = op.mul(X, precision="bf16x3")
+    e32, e3 = rel(Y32, Y64), rel(Y3, Y64)
+    assert e3 < 2e-6 and e3 < 3 * e32, (e3, e32)
 
 
 @pytest.mark.parametrize("k", [1, 3, 8, 64, 128])
