@@ -26,7 +26,7 @@ EXPORTS = [
     "bie_near_destroy", "bie_geom_create", "bie_geom_create_from_mesh", "bie_geom_info", "bie_geom_stream",
     "bie_geom_destroy", "bie_matvec", "bie_matvec_device", "bie_rhs_point", "bie_rhs_point_device",
     "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve",
-    "bie_solve_device", "bie_profile_enable", "bie_profile_read",
+    "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
 ]
 
 
@@ -117,6 +117,7 @@ def lib():
         "bie_solve_device": (i, [_vp, _vp, _vp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats), _vp]),
         "bie_profile_enable": (i, [_vp, i]),
         "bie_profile_read": (i, [_vp, i, C.POINTER(KernelTime)]),
+        "bie_dt_apply_static": (i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, i64, _vp, C.c_int32, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

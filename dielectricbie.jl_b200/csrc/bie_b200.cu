@@ -313,6 +313,12 @@ int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int3
     });
 }
 
+int bie_dt_apply_static(const double* x, const double* y, const double* z, const double* nx, const double* ny,
+                        const double* nz, const double* w, int64_t n, const double* X, int32_t k, double* Y,
+                        void* stream) {
+    return guarded([&] { bie::dt_apply_static(x, y, z, nx, ny, nz, w, n, X, k, Y, (cudaStream_t)stream); });
+}
+
 int bie_rhs_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* F) {
     return guarded([&] {
         REQUIRE(g && src && q && eps_src && F && k >= 1, "rhs_point: bad argument");

@@ -49,4 +49,10 @@ int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_sol
 int solve_device(bie_geom* g, const double* dF, double* dSigma, int k, const bie_solve_opts& o, bie_stats* st,
                  cudaStream_t s);
 
+// noalloc.cu: direct sum with the split partials in a fixed device array.
+int64_t dt_apply_static_max_nodes();
+void dt_apply_static(const double* x, const double* y, const double* z, const double* nx, const double* ny,
+                     const double* nz, const double* w, int64_t n, const double* X, int k, double* Y,
+                     cudaStream_t s);
+
 }  // namespace bie

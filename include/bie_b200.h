@@ -152,6 +152,29 @@ int bie_matvec(bie_geom* g, const double* X, double* Y, int32_t k, int32_t preci
 int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int32_t precision, uint32_t flags,
                       void* stream);
 
+/* No counterpart in the reference. FP64 direct sum of the adjoint double layer
+ * without near-field correction or diagonal, that allocates no device memory:
+ *   Y[i][c] = 1/(4 pi) sum_{j != i} n_i.(x_i - y_j)/|x_i - y_j|^3 w_j X[j][c].
+ * It is for callers that cannot let a library allocate: host runtimes whose pool
+ * allocator owns the device memory (Julia's CUDA.jl, PyTorch's caching allocator),
+ * where a foreign cudaMalloc can fail while the pool holds free memory, and
+ * latency-bound services that reserve memory at start-up, since cudaMalloc and
+ * cudaFree synchronise the device. The split partials live in a fixed 32 MiB
+ * device array inside the library (held by every device the library runs it on,
+ * until the process exits); the caller passes all inputs and outputs as device
+ * pointers on the current device: node coordinates x, y, z, unit normals nx, ny,
+ * nz and weights w (n each), X and Y node-major n x k (Y must not overlap X).
+ * Limit: n <= 4,194,304 nodes; larger n is rejected with BIE_EINVAL before any
+ * device work. The first call on a device looks up the array's address; make that
+ * first call before any stream capture. Calls share the array: every partial a
+ * call reads is written earlier in the same call, so nothing needs clearing, but
+ * calls that overlap on the GPU (other streams, other threads) race on it and
+ * must be serialised by the caller. Work is ordered on `stream` (NULL = the
+ * default stream); the call returns without synchronising. */
+int bie_dt_apply_static(const double* x, const double* y, const double* z, const double* nx, const double* ny,
+                        const double* nz, const double* w, int64_t n, const double* X, int32_t k, double* Y,
+                        void* stream);
+
 /* F[:, c] = rhs_dielectric_box3d(itf, PointSource(src[:, c], q[c]), eps_src[c])
  * (src/solver/dielectric_box3d.jl:95-104). src 3 x k, F N x k (host). */
 int bie_rhs_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* F);
