@@ -235,47 +235,95 @@ __device__ __forceinline__ void split_pieces(float a, float b, uint32_t* out) {
     }
 }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): one instruction applies the same
+// round-to-nearest operation to two sources.
+__device__ __forceinline__ uint64_t f2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 f2u(uint64_t r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// split_pieces on a packed pair (the remainders are formed with one packed subtract).
+template <int NP>
+__device__ __forceinline__ void split_pieces2(uint64_t x, uint32_t* out) {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const float2 xu = f2u(x);
+        const uint32_t w = pack_bf16(xu.x, xu.y);
+        out[p] = w;
+        if (p + 1 < NP) x = f2sub(x, f2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u)));
+    }
+}
+
 // One thread's share of a row of a chunk's kernel tile: 64 / NQ sources (8-source
-// groups gq0 .. gq0 + 8 / NQ - 1), processed 16 at a time. AXIS: the rows of this
-// warp have normal +-e_a for one axis a (sign applied in the epilogue); ca holds the
-// source coordinates along a and cb, cc the other two, ta, tb, tc the target's in
-// the same order, so one code path serves the three axes. !AXIS: general normal
-// (n0, n1, n2), with (ca, cb, cc) = (x, y, z).
+// groups gq0 .. gq0 + 8 / NQ - 1), processed 16 at a time as 8 packed pairs. AXIS:
+// the rows of this warp have normal +-e_a for one axis a (sign applied in the
+// epilogue); ca holds the source coordinates along a and cb, cc the other two,
+// t2a, t2b, t2c the target's in the same order (duplicated into both halves of a
+// pair), so one code path serves the three axes. !AXIS: general normal (n2x, n2y,
+// n2z duplicated), with (ca, cb, cc) = (x, y, z).
 template <bool AXIS, int NP, int NQ>
 __device__ __forceinline__ void gen_row_part(const float* __restrict__ ca, const float* __restrict__ cb,
-                                             const float* __restrict__ cc, float ta, float tb, float tc, float n0,
-                                             float n1, float n2, int gq0, bool self, int64_t j0, int64_t i,
-                                             uint8_t* Astage, uint32_t a_bytes, uint32_t row_off, uint32_t rsw) {
+                                             const float* __restrict__ cc, uint64_t t2a, uint64_t t2b,
+                                             uint64_t t2c, uint64_t n2x, uint64_t n2y, uint64_t n2z, int gq0,
+                                             bool self, int64_t j0, int64_t i, uint8_t* Astage, uint32_t a_bytes,
+                                             uint32_t row_off, uint32_t rsw) {
 #pragma unroll 1
     for (int gq = gq0; gq < gq0 + 8 / NQ; gq += 2) {
-        float v[16];
+        uint64_t v[8];  // kernel values of sources gq * 8 + 2 m, + 1
 #pragma unroll
         for (int e4 = 0; e4 < 4; ++e4) {
             const int b = gq * 8 + e4 * 4;
             const float4 A4 = *reinterpret_cast<const float4*>(ca + b);
             const float4 B4 = *reinterpret_cast<const float4*>(cb + b);
             const float4 C4 = *reinterpret_cast<const float4*>(cc + b);
-            const float sa[4] = {A4.x, A4.y, A4.z, A4.w}, sb[4] = {B4.x, B4.y, B4.z, B4.w},
-                        sc[4] = {C4.x, C4.y, C4.z, C4.w};
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const float da = ta - sa[e], db = tb - sb[e], dc = tc - sc[e];
-                const float r2 = fmaf(da, da, fmaf(db, db, dc * dc));
-                const float ri = rsqrt_mufu(r2);
-                const float dn = AXIS ? da : fmaf(n0, da, fmaf(n1, db, n2 * dc));
-                v[e4 * 4 + e] = (dn * ri) * (ri * ri);
+            for (int h = 0; h < 2; ++h) {
+                const uint64_t sa = h ? f2(A4.z, A4.w) : f2(A4.x, A4.y);
+                const uint64_t sb = h ? f2(B4.z, B4.w) : f2(B4.x, B4.y);
+                const uint64_t sc = h ? f2(C4.z, C4.w) : f2(C4.x, C4.y);
+                const uint64_t da = f2sub(t2a, sa), db = f2sub(t2b, sb), dc = f2sub(t2c, sc);
+                const uint64_t r2 = f2fma(da, da, f2fma(db, db, f2mul(dc, dc)));
+                const float2 r2u = f2u(r2);
+                const uint64_t ri = f2(rsqrt_mufu(r2u.x), rsqrt_mufu(r2u.y));
+                const uint64_t dn = AXIS ? da : f2fma(n2x, da, f2fma(n2y, db, f2mul(n2z, dc)));
+                v[e4 * 2 + h] = f2mul(f2mul(dn, ri), f2mul(ri, ri));
             }
         }
         if (self) {
 #pragma unroll
-            for (int e = 0; e < 16; ++e)
-                if (j0 + gq * 8 + e == i) v[e] = 0.f;
+            for (int m = 0; m < 8; ++m) {
+                float2 u = f2u(v[m]);
+                if (j0 + gq * 8 + 2 * m == i) u.x = 0.f;
+                if (j0 + gq * 8 + 2 * m + 1 == i) u.y = 0.f;
+                v[m] = f2(u.x, u.y);
+            }
         }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             uint32_t w[4][NP];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) split_pieces<NP>(v[8 * h + 2 * e], v[8 * h + 2 * e + 1], w[e]);
+            for (int e = 0; e < 4; ++e) split_pieces2<NP>(v[4 * h + e], w[e]);
             const uint32_t off = row_off + ((((uint32_t)(gq + h)) ^ rsw) << 4);
 #pragma unroll
             for (int p = 0; p < NP; ++p)
@@ -389,6 +437,9 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
         const float ta = a1 == 0 ? tcrd[0] : (a1 == 1 ? tcrd[1] : tcrd[2]);
         const float tb = a2 == 0 ? tcrd[0] : (a2 == 1 ? tcrd[1] : tcrd[2]);
         const float tc = a3 == 0 ? tcrd[0] : (a3 == 1 ? tcrd[1] : tcrd[2]);
+        const uint64_t t2a = f2(ta, ta), t2b = f2(tb, tb), t2c = f2(tc, tc);
+        const uint64_t t2x = f2(xi, xi), t2y = f2(yi, yi), t2z = f2(zi, zi);
+        const uint64_t n2x = f2(n0, n0), n2y = f2(n1, n1), n2z = f2(n2, n2);
         const uint32_t row_off = (uint32_t)r * 128u;
         const uint32_t rsw = (uint32_t)(r & 7);
         const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
@@ -433,11 +484,11 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
             const bool self = (i >= j0) && (i < j0 + KC);  // this chunk holds the target's own node
             const int gq0 = qt * (8 / NQ);
             if (ax < 3)
-                gen_row_part<true, NP, NQ>(cs + oa, cs + ob, cs + oc, ta, tb, tc, n0, n1, n2, gq0, self, j0, i, As,
-                                           a_bytes, row_off, rsw);
+                gen_row_part<true, NP, NQ>(cs + oa, cs + ob, cs + oc, t2a, t2b, t2c, n2x, n2y, n2z, gq0, self, j0, i,
+                                           As, a_bytes, row_off, rsw);
             else
-                gen_row_part<false, NP, NQ>(cs, cs + KC, cs + 2 * KC, xi, yi, zi, n0, n1, n2, gq0, self, j0, i, As,
-                                            a_bytes, row_off, rsw);
+                gen_row_part<false, NP, NQ>(cs, cs + KC, cs + 2 * KC, t2x, t2y, t2z, n2x, n2y, n2z, gq0, self, j0, i,
+                                            As, a_bytes, row_off, rsw);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&full_a[s]);
             mbar_arrive(&crd_empty[sc]);
