@@ -262,94 +262,167 @@ __global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int
 // c = t % kt and the rows [g R, g R + R) of group g = t / kt: every slab value it
 // loads feeds R FMAs, and the R block values are warp-wide broadcasts. Then
 //   Y[i][c] = (1/4pi) sum_s part[s][i][c] + sum_b B . (p X) + t_i p_i X[i][c].
-constexpr int kKT = 64;     // column tile of the block-row combine
-constexpr int kRmax = 16;   // rows per thread (nb <= (256 / kt) * kRmax)
-template <int R>
-__global__ void __launch_bounds__(256) k_combine_panel(int64_t n, int k, const double* __restrict__ part, int nsplit,
-                                                       const double* __restrict__ X, const double* __restrict__ pre,
-                                                       const double* __restrict__ diag,
-                                                       const int32_t* __restrict__ rowptr,
-                                                       const int32_t* __restrict__ col,
-                                                       const double* __restrict__ val, int nb,
-                                                       double* __restrict__ Y) {
-    constexpr int PF = 16;  // staged elements per thread and array (nb <= 64, kt <= 64)
-    extern __shared__ double smc[];
+// ---------------------------------------------------------------------------
+// K4 (block-row form): one CTA per (target panel P, 32-column tile). The BSR
+// blocks of the panel's row, C_b (nb x nb, column-major), multiply the slabs
+// p .* X[source panel of b] on the FP64 tensor path (mma.sync m8n8k4 f64; a
+// warp owns one 8-column n-tile and the panel's MT 8-row m-tiles); blocks and
+// slabs are double-buffered in shared memory by cp.async. The epilogue adds the
+// split partials (times 1/(4 pi)) and the diagonal term:
+//   Y[i][c] = (1/4pi) sum_s part[s][i][c] + sum_b (C_b (p X)[col_b])[i][c] + t_i p_i X[i][c]
+// Replaces the CSC SpMV / sparse mat-mat of laplace3d_DT_fmm3d_corrected and
+// BatchedDielectricOperator (src/kernel/laplace3d_near.jl:395-419,
+// src/solver/multi_rhs.jl:103-136).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+constexpr int kCombTile = 32;  // columns per CTA
+constexpr int kCombLDX = 36;   // slab row stride (doubles): 32 + 4, conflict-free fragment loads
+
+// Shared memory of the block-row combine for nb-row panels.
+inline size_t combine_smem_bytes(int nb) {
+    const int mt = (nb + 7) / 8, kp = ((nb + 3) / 4) * 4;
+    const int ldc = mt * 8 + 4;
+    return sizeof(double) * (2 * (size_t)kp * ldc + 2 * (size_t)kp * kCombLDX + 2 * (size_t)kp);
+}
+
+template <int MT>
+__global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const double* __restrict__ part, int nsplit,
+                                                      const double* __restrict__ X, const double* __restrict__ pre,
+                                                      const double* __restrict__ diag,
+                                                      const int32_t* __restrict__ rowptr,
+                                                      const int32_t* __restrict__ col,
+                                                      const double* __restrict__ val, int nb,
+                                                      double* __restrict__ Y) {
+    // column stride of a staged block: MT * 8 rows + 4 (= 4 or 12 mod 16 doubles, so the
+    // four k-rows a half-warp reads fall in distinct banks)
+    constexpr int LDC = MT * 8 + 4;
+    constexpr int LDX = kCombLDX;
+    const int KS = (nb + 3) / 4, KP = KS * 4;
+    extern __shared__ __align__(16) double smd[];
+    double* sC = smd;                   // [2][KP][LDC], sC[q * LDC + r] = C_b[r][q]
+    double* sX = sC + 2 * KP * LDC;     // [2][KP][LDX], sX[q * LDX + cc] = X[col_b * nb + q][c0 + cc]
+    double* sP = sX + 2 * KP * LDX;     // [2][KP] preconditioner of the slab rows
     const int P = blockIdx.x;
+    const int c0 = blockIdx.y * kCombTile;
+    const int kt = min(kCombTile, k - c0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row0 = (int64_t)P * nb;
-    const int nb2 = nb * nb;
-    const int64_t tot = n * (int64_t)k;
     const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
-    const int T = blockDim.x;
-    for (int c0 = 0; c0 < k; c0 += kKT) {
-        const int kt = min(kKT, k - c0);
-        const int G = T / kt;
-        const int c = threadIdx.x % kt, grp = threadIdx.x / kt;
-        const int r0 = grp * R;
-        // rows of this thread: r0 .. r0 + R - 1, valid while < nb (sv is padded to a multiple of R rows)
-        const bool act = grp < G && r0 < nb;
-        const int ldv = ((nb + R - 1) / R) * R;  // padded leading dimension of the staged block
-        const int nv = nb * ldv, nxs = nb * kt;
-        double* sv = smc;        // [nb][ldv], sv[q * ldv + r]
-        double* sx = smc + nv;   // [nb][kt]
-        double acc[R];
-#pragma unroll
-        for (int m = 0; m < R; ++m) acc[m] = 0.0;
-        // register staging of one block: its values and the slab of (p X) it multiplies
-        double pv[PF], px[PF];
-        auto fetch = [&](int b) {
-            const double* vb = val + (int64_t)b * nb2;
-            const int64_t base = (int64_t)col[b] * nb;
-#pragma unroll
-            for (int u = 0; u < PF; ++u) {
-                const int e = threadIdx.x + u * T;
-                if (e < nv) {
-                    const int q = e / ldv, r = e - q * ldv;
-                    pv[u] = r < nb ? vb[q * nb + r] : 0.0;
-                }
-                if (e < nxs) {
-                    const int q = e / kt, cc = e - q * kt;
-                    const double x = X[(base + q) * k + c0 + cc];
-                    px[u] = pre ? pre[base + q] * x : x;
-                }
+    // padding rows/columns stay zero: the copies below write only the live part
+    for (int e = threadIdx.x; e < 2 * KP * (LDC + LDX + 1); e += blockDim.x) smd[e] = 0.0;
+    __syncthreads();
+
+    const bool v16 = (nb & 1) == 0;  // 16-byte copies of block columns (the blocks are 16-byte aligned)
+    const bool x16 = (k & 1) == 0 && (kt & 1) == 0 &&  // and of slab rows (c0 is even)
+                     (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+    auto issue = [&](int b, int st) {
+        const double* vb = val + (int64_t)b * nb * nb;
+        double* dC = sC + st * KP * LDC;
+        if (v16) {
+            const int h = nb >> 1;
+            for (int e = threadIdx.x; e < nb * h; e += blockDim.x) {
+                const int q = e / h, r = (e - q * h) * 2;
+                cp_async16(dC + q * LDC + r, vb + q * nb + r);
             }
-        };
-        if (b0 < b1) fetch(b0);
-        for (int b = b0; b < b1; ++b) {
-            __syncthreads();  // previous block consumed
-#pragma unroll
-            for (int u = 0; u < PF; ++u) {
-                const int e = threadIdx.x + u * T;
-                if (e < nv) sv[e] = pv[u];
-                if (e < nxs) sx[e] = px[u];
-            }
-            __syncthreads();
-            if (b + 1 < b1) fetch(b + 1);  // next block's loads in flight during the math
-            if (act) {
-#pragma unroll 4
-                for (int q = 0; q < nb; ++q) {
-                    const double x = sx[q * kt + c];
-                    const double* v = sv + q * ldv + r0;
-#pragma unroll
-                    for (int m = 0; m < R; ++m) acc[m] = fma(v[m], x, acc[m]);
-                }
+        } else {
+            for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+                const int q = e / nb, r = e - q * nb;
+                cp_async8(dC + q * LDC + r, vb + q * nb + r);
             }
         }
-        if (act) {
-#pragma unroll
-            for (int m = 0; m < R; ++m) {
-                const int r = r0 + m;
-                if (r < nb) {
-                    const int64_t i = row0 + r;
-                    const int64_t e = i * k + c0 + c;
-                    double s = 0.0;
-                    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
-                    s = s * kInv4Pi + acc[m];
-                    if (diag) s += diag[i] * (pre ? pre[i] : 1.0) * X[e];
-                    Y[e] = s;
-                }
+        const int64_t base = (int64_t)col[b] * nb;
+        double* dX = sX + st * KP * LDX;
+        if (x16) {
+            const int h = kt >> 1;
+            for (int e = threadIdx.x; e < nb * h; e += blockDim.x) {
+                const int q = e / h, cc = (e - q * h) * 2;
+                cp_async16(dX + q * LDX + cc, X + (base + q) * k + c0 + cc);
+            }
+        } else {
+            for (int e = threadIdx.x; e < nb * kt; e += blockDim.x) {
+                const int q = e / kt, cc = e - q * kt;
+                cp_async8(dX + q * LDX + cc, X + (base + q) * k + c0 + cc);
             }
         }
-        __syncthreads();  // smem reused by the next column tile
+        if (pre)
+            for (int q = threadIdx.x; q < nb; q += blockDim.x) cp_async8(sP + st * KP + q, pre + base + q);
+        cp_async_commit();
+    };
+
+    // warps to (n-tile, m-tile subset): with fewer than four n-tiles the warps share
+    // an n-tile and split its m-tiles
+    const int ntiles = (kt + 7) / 8;
+    const int nw = ntiles >= 4 ? 4 : ntiles;  // distinct n-tiles in use
+    const int mstep = 4 / nw;                 // 1, 2 or 4 (nw = 3: one warp idle)
+    const int nt = warp % nw, moff = warp / nw;
+    const bool wact = moff < mstep;
+    double acc[MT][2];
+#pragma unroll
+    for (int m = 0; m < MT; ++m) acc[m][0] = acc[m][1] = 0.0;
+
+    if (b0 < b1) issue(b0, 0);
+    for (int b = b0; b < b1; ++b) {
+        const int st = (b - b0) & 1;
+        if (b + 1 < b1) {
+            issue(b + 1, st ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (wact) {
+            const double* cC = sC + st * KP * LDC + (lane >> 2);
+            const double* cX = sX + st * KP * LDX + 8 * nt + (lane >> 2);
+            const double* cP = sP + st * KP;
+            for (int ks = 0; ks < KS; ++ks) {
+                const int q = 4 * ks + (lane & 3);
+                double bv = cX[q * LDX];
+                if (pre) bv *= cP[q];
+#pragma unroll
+                for (int m = 0; m < MT; ++m)
+                    if (m % mstep == moff) dmma884(acc[m][0], acc[m][1], cC[q * LDC + 8 * m], bv);
+            }
+        }
+        __syncthreads();  // stage st is refilled two iterations later
+    }
+
+    if (!wact) return;
+    const int64_t tot = n * (int64_t)k;
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+        if (m % mstep != moff) continue;
+        const int r = 8 * m + (lane >> 2);
+        if (r >= nb) continue;
+        const int64_t i = row0 + r;
+        const double dgi = diag ? diag[i] * (pre ? pre[i] : 1.0) : 0.0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c = c0 + 8 * nt + 2 * (lane & 3) + h;
+            if (c >= c0 + kt) continue;
+            const int64_t e = i * k + c;
+            double sp = 0.0;
+            for (int p = 0; p < nsplit; ++p) sp += part[(int64_t)p * tot + e];
+            double y = sp * kInv4Pi + acc[m][h];
+            if (diag) y += dgi * X[e];
+            Y[e] = y;
+        }
     }
 }
 

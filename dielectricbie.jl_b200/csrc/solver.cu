@@ -318,64 +318,41 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
                                 : 0.0) +
                           (double)g->n * k * 8 * (2 + sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
     Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
-    const int kt0 = std::min(k, kKT);
-    const int G0 = 256 / kt0;
-    const int R0 = (g->nb + G0 - 1) / G0;
-    if (g->nb > 0 && g->nb <= 64 && (int64_t)g->npanels * g->nb == g->n && R0 <= kRmax) {
-        // shared memory: the padded block (nb x G R) and the slab (nb x kt) of the widest tile
-        const size_t sm = sizeof(double) * ((size_t)g->nb * G0 * R0 + (size_t)g->nb * kt0);
+    const double* dgp = dg ? g->diag.as<double>() : nullptr;
+    const int32_t* rp = corr ? g->rowptr.as<int32_t>() : nullptr;
+    const int32_t* cl = corr ? g->col.as<int32_t>() : nullptr;
+    const double* vl = corr ? g->val.as<double>() : nullptr;
+    const int mt = (g->nb + 7) / 8;
+    if (g->nb > 0 && mt <= 8 && (int64_t)g->npanels * g->nb == g->n) {
+        const size_t sm = combine_smem_bytes(g->nb);
         static bool attr = false;
         if (!attr) {
-            const void* fs[] = {(const void*)k_combine_panel<1>, (const void*)k_combine_panel<2>,
-                                (const void*)k_combine_panel<3>, (const void*)k_combine_panel<4>,
-                                (const void*)k_combine_panel<6>, (const void*)k_combine_panel<8>,
-                                (const void*)k_combine_panel<9>, (const void*)k_combine_panel<12>,
-                                (const void*)k_combine_panel<16>};
+            const void* fs[] = {(const void*)k_combine_dmma<1>, (const void*)k_combine_dmma<2>,
+                                (const void*)k_combine_dmma<3>, (const void*)k_combine_dmma<4>,
+                                (const void*)k_combine_dmma<5>, (const void*)k_combine_dmma<6>,
+                                (const void*)k_combine_dmma<7>, (const void*)k_combine_dmma<8>};
             for (const void* f : fs)
-                BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+                BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
             attr = true;
         }
-        // the column tiles after the first are narrower or equal: the same R bound holds for them only if
-        // k is a multiple of kKT or k < kKT; otherwise fall through to the generic kernel
-        const bool uniform = k <= kKT || k % kKT == 0;
-        int Rk = R0 <= 1 ? 1 : R0 <= 2 ? 2 : R0 <= 3 ? 3 : R0 <= 4 ? 4 : R0 <= 6 ? 6 : R0 <= 8 ? 8 : R0 <= 9 ? 9
-                 : R0 <= 12 ? 12 : 16;
-        if (uniform) {
-            const double* dgp = dg ? g->diag.as<double>() : nullptr;
-            const int32_t* rp = corr ? g->rowptr.as<int32_t>() : nullptr;
-            const int32_t* cl = corr ? g->col.as<int32_t>() : nullptr;
-            const double* vl = corr ? g->val.as<double>() : nullptr;
-            const size_t ldv = (size_t)((g->nb + Rk - 1) / Rk) * Rk;
-            const size_t smr = sizeof(double) * ((size_t)g->nb * ldv + (size_t)g->nb * kt0);
-            (void)sm;
-#define BIE_COMB(RR)                                                                                            \
-    k_combine_panel<RR><<<(unsigned)g->npanels, 256, smr, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, pre, \
-                                                               dgp, rp, cl, vl, g->nb, Y)
-            switch (Rk) {
-                case 1: BIE_COMB(1); break;
-                case 2: BIE_COMB(2); break;
-                case 3: BIE_COMB(3); break;
-                case 4: BIE_COMB(4); break;
-                case 6: BIE_COMB(6); break;
-                case 8: BIE_COMB(8); break;
-                case 9: BIE_COMB(9); break;
-                case 12: BIE_COMB(12); break;
-                default: BIE_COMB(16); break;
-            }
-#undef BIE_COMB
-        } else {
-            k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
-                                                      dg ? g->diag.as<double>() : nullptr,
-                                                      corr ? g->rowptr.as<int32_t>() : nullptr,
-                                                      corr ? g->col.as<int32_t>() : nullptr,
-                                                      corr ? g->val.as<double>() : nullptr, g->nb, Y, k);
+        dim3 grid((unsigned)g->npanels, (unsigned)((k + kCombTile - 1) / kCombTile));
+#define BIE_COMB(MT)                                                                                            \
+    k_combine_dmma<MT><<<grid, 128, sm, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, pre, dgp, rp, cl, vl, \
+                                             g->nb, Y)
+        switch (mt) {
+            case 1: BIE_COMB(1); break;
+            case 2: BIE_COMB(2); break;
+            case 3: BIE_COMB(3); break;
+            case 4: BIE_COMB(4); break;
+            case 5: BIE_COMB(5); break;
+            case 6: BIE_COMB(6); break;
+            case 7: BIE_COMB(7); break;
+            default: BIE_COMB(8); break;
         }
+#undef BIE_COMB
     } else {
-        k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre,
-                                                  dg ? g->diag.as<double>() : nullptr,
-                                                  corr ? g->rowptr.as<int32_t>() : nullptr,
-                                                  corr ? g->col.as<int32_t>() : nullptr,
-                                                  corr ? g->val.as<double>() : nullptr, g->nb, Y, k);
+        k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre, dgp, rp, cl,
+                                                  vl, g->nb, Y, k);
     }
     BIE_CK(cudaGetLastError());
 }
