@@ -465,37 +465,75 @@ __global__ void k_nodemajor_to_colmajor(const double* __restrict__ B, int64_t n,
 // K7: device GMRES building blocks (FP64). Multi-column vectors node-major
 // (n x k); each of the k columns runs its own Arnoldi process.
 // ---------------------------------------------------------------------------
-// partial[v][blk][c] = sum_{i in blk rows} A_v[i][c] * B[i][c]  for v < nv
-// (A_v = A + v * strideA). blockDim.x = multiple of k (threads t, t + k, ... share c).
-__global__ void k_dots_partial(const double* __restrict__ A, int64_t strideA, int nv, const double* __restrict__ B,
-                               int64_t n, int k, int64_t rows_per_blk, double* __restrict__ partial, int nblk) {
+// Column dot products, one CTA per (row block, vector v): partial[blk][v][c] = sum over
+// the block's rows of A_v[i][c] B[i][c], A_v = A + v * strideA. blockDim.x = k * groups
+// (groups a power of two): thread t owns column t % k and every groups-th row.
+__global__ void k_dots_blk(const double* __restrict__ A, int64_t strideA, int nv, const double* __restrict__ B,
+                           int64_t n, int k, int64_t rows_per_blk, double* __restrict__ partial) {
     extern __shared__ double red[];
+    const int groups = blockDim.x / k;
+    const int c = threadIdx.x % k, grp = threadIdx.x / k;
     const int v = blockIdx.y;
     const double* Av = A + (int64_t)v * strideA;
     const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk;
     const int64_t r1 = min(n, r0 + rows_per_blk);
-    const int64_t e0 = r0 * k, e1 = r1 * k;
-    double s = 0.0;
-    for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) s = fma(Av[e], B[e], s);
-    red[threadIdx.x] = s;
+    double sacc = 0.0;
+    for (int64_t r = r0 + grp; r < r1; r += groups) sacc = fma(Av[r * k + c], B[r * k + c], sacc);
+    red[threadIdx.x] = sacc;
     __syncthreads();
-    // reduce the groups {c, c + k, c + 2k, ...}; blockDim.x / k is a power of two
-    for (int h = (int)(blockDim.x / k) / 2; h > 0; h >>= 1) {
+    for (int h = groups / 2; h > 0; h >>= 1) {
         if (threadIdx.x < (unsigned)(h * k)) red[threadIdx.x] += red[threadIdx.x + h * k];
         __syncthreads();
     }
-    if (threadIdx.x < (unsigned)k) partial[((int64_t)v * nblk + blockIdx.x) * k + threadIdx.x] = red[threadIdx.x];
+    if (threadIdx.x < (unsigned)k)
+        partial[(int64_t)blockIdx.x * nv * k + (int64_t)v * k + threadIdx.x] = red[threadIdx.x];
 }
 
-// out[v][c] = sum_blk partial[v][blk][c]; mode 0: assign, 1: accumulate, 2: assign sqrt
-__global__ void k_dots_finish(const double* __restrict__ partial, int nv, int nblk, int k, double* __restrict__ out,
-                              int mode) {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nv * k) return;
-    int v = e / k, c = e - v * k;
-    double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += partial[((int64_t)v * nblk + b) * k + c];
-    out[e] = mode == 1 ? out[e] + s : (mode == 2 ? sqrt(s) : s);
+// W[i][c] -= sum_{v < nv} V_v[i][c] h[v][c], then partial[blk][c] = sum over the block's
+// rows of W[i][c]^2 (the second Gram-Schmidt pass fused with the column norm).
+__global__ void k_gs_update_norm(double* __restrict__ W, const double* __restrict__ V, int64_t strideV, int nv,
+                                 const double* __restrict__ h, int64_t n, int k, int64_t rows_per_blk,
+                                 double* __restrict__ partial) {
+    extern __shared__ double red[];
+    const int groups = blockDim.x / k;
+    const int c = threadIdx.x % k, grp = threadIdx.x / k;
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_blk;
+    const int64_t r1 = min(n, r0 + rows_per_blk);
+    double sacc = 0.0;
+    if (grp < groups)
+        for (int64_t r = r0 + grp; r < r1; r += groups) {
+            const int64_t e = r * k + c;
+            double w = W[e];
+            for (int v = 0; v < nv; ++v) w = fma(-V[(int64_t)v * strideV + e], h[v * k + c], w);
+            W[e] = w;
+            sacc = fma(w, w, sacc);
+        }
+    red[threadIdx.x] = sacc;
+    __syncthreads();
+    for (int hh = groups / 2; hh > 0; hh >>= 1) {
+        if (threadIdx.x < (unsigned)(hh * k)) red[threadIdx.x] += red[threadIdx.x + hh * k];
+        __syncthreads();
+    }
+    if (threadIdx.x < (unsigned)k) partial[(int64_t)blockIdx.x * k + threadIdx.x] = red[threadIdx.x];
+}
+
+// out[e] = sum_blk partial[blk][e] for e < nout, in a fixed order (8 outputs x 32 block
+// subsets per CTA); mode 0: assign, 1: accumulate, 2: assign the square root.
+__global__ void __launch_bounds__(256) k_dots_finish(const double* __restrict__ partial, int nblk, int64_t nout,
+                                                     double* __restrict__ out, int mode) {
+    __shared__ double red[32][8];
+    const int o = threadIdx.x & 7, sub = threadIdx.x >> 3;
+    const int64_t e = (int64_t)blockIdx.x * 8 + o;
+    double sacc = 0.0;
+    if (e < nout)
+        for (int b = sub; b < nblk; b += 32) sacc += partial[(int64_t)b * nout + e];
+    red[sub][o] = sacc;
+    __syncthreads();
+    if (threadIdx.x < 8 && e < nout) {
+        double t = 0.0;
+        for (int q = 0; q < 32; ++q) t += red[q][o];
+        out[e] = mode == 1 ? out[e] + t : (mode == 2 ? sqrt(t) : t);
+    }
 }
 
 // W[i][c] -= sum_{v < nv} V_v[i][c] h[v][c]
@@ -531,6 +569,7 @@ __global__ void k_axpby(double a, const double* __restrict__ X, double b, double
 // Givens step of iteration j for every active column (one thread per column).
 // R: [(m+1) x (m+1) x k] column j holds h[0..j+1]; cs/sn: [m x k]; gv: [(m+1) x k].
 __global__ void k_givens(double* __restrict__ R, const double* __restrict__ h /*[(j+1) x k]*/,
+                         const double* __restrict__ h2 /*[(j+1) x k], second Gram-Schmidt pass*/,
                          const double* __restrict__ hnorm /*[k]*/, double* __restrict__ cs, double* __restrict__ sn,
                          double* __restrict__ gv, int* __restrict__ active, int* __restrict__ jlast,
                          const double* __restrict__ eps, double* __restrict__ resid, int j, int m1, int k) {
@@ -538,7 +577,7 @@ __global__ void k_givens(double* __restrict__ R, const double* __restrict__ h /*
     if (c >= k) return;
     if (!active[c]) return;
     double* Rj = R + ((int64_t)j * m1) * k;  // column j: Rj[i * k + c]
-    for (int i = 0; i <= j; ++i) Rj[i * k + c] = h[i * k + c];
+    for (int i = 0; i <= j; ++i) Rj[i * k + c] = h[i * k + c] + h2[i * k + c];
     Rj[(j + 1) * k + c] = hnorm[c];
     for (int i = 0; i < j; ++i) {
         double a = Rj[i * k + c], b = Rj[(i + 1) * k + c];

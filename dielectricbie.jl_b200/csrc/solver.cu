@@ -363,18 +363,25 @@ struct DotPlan {
     int64_t rows_per_blk;
 };
 
+// Row blocks of the column reductions: about 2048 CTAs over all vectors, each with
+// at least 4 elements per thread.
 DotPlan dot_plan(int64_t n, int k, int nv) {
+    if (k > 256) throw Error(BIE_EUNSUPPORTED, "more than 256 right-hand sides per solve");
     int groups = 1;
     while (k * groups * 2 <= 256) groups *= 2;
     DotPlan p;
     p.bs = k * groups;
-    if (p.bs < 32 && k <= 256) p.bs = k * groups;  // k > 256 handled by the caller (unsupported)
-    int64_t elems = n * (int64_t)k;
-    int64_t nblk = std::max<int64_t>(1, std::min<int64_t>(1024 / std::max(1, nv) + 1, (elems + p.bs * 16 - 1) / (p.bs * 16)));
-    nblk = std::min<int64_t>(nblk, n);
+    const int64_t elems = n * (int64_t)k;
+    int64_t nblk = std::min<int64_t>((2048 + nv - 1) / std::max(1, nv), (elems + 4 * p.bs - 1) / (4 * p.bs));
+    nblk = std::max<int64_t>(1, std::min<int64_t>(nblk, n));
     p.rows_per_blk = (n + nblk - 1) / nblk;
     p.nblk = (int)((n + p.rows_per_blk - 1) / p.rows_per_blk);
     return p;
+}
+
+void dots_finish(bie_geom* g, int nblk, int64_t nout, double* out, int mode, cudaStream_t s) {
+    k_dots_finish<<<(unsigned)((nout + 7) / 8), 256, 0, s>>>(g->dpart.as<double>(), nblk, nout, out, mode);
+    BIE_CK(cudaGetLastError());
 }
 
 // out[v][c] = sum_i A_v[i][c] B[i][c] for v < nv (mode: 0 assign, 1 accumulate, 2 sqrt)
@@ -382,13 +389,23 @@ void dots(bie_geom* g, const double* A, int64_t strideA, int nv, const double* B
           cudaStream_t s) {
     DotPlan p = dot_plan(g->n, k, nv);
     g->dpart.ensure(sizeof(double) * (size_t)p.nblk * nv * k);
-    dim3 grid(p.nblk, nv);
     Prof pf(g, BIE_KERNEL_KRYLOV, s, 2);
-    k_dots_partial<<<grid, p.bs, p.bs * sizeof(double), s>>>(A, strideA, nv, B, g->n, k, p.rows_per_blk,
-                                                            g->dpart.as<double>(), p.nblk);
+    k_dots_blk<<<dim3(p.nblk, nv), p.bs, p.bs * sizeof(double), s>>>(A, strideA, nv, B, g->n, k, p.rows_per_blk,
+                                                                    g->dpart.as<double>());
     BIE_CK(cudaGetLastError());
-    k_dots_finish<<<grid1(nv * k), 256, 0, s>>>(g->dpart.as<double>(), nv, p.nblk, k, out, mode);
+    dots_finish(g, p.nblk, (int64_t)nv * k, out, mode, s);
+}
+
+// W -= sum_v V_v h[v] (columnwise), then out[c] = |W[:, c]|
+void gs_update_norm(bie_geom* g, double* W, const double* V, int64_t strideV, int nv, const double* h, int k,
+                    double* out, cudaStream_t s) {
+    DotPlan p = dot_plan(g->n, k, 1);
+    g->dpart.ensure(sizeof(double) * (size_t)p.nblk * k);
+    Prof pf(g, BIE_KERNEL_KRYLOV, s, 2);
+    k_gs_update_norm<<<p.nblk, p.bs, p.bs * sizeof(double), s>>>(W, V, strideV, nv, h, g->n, k, p.rows_per_blk,
+                                                                g->dpart.as<double>());
     BIE_CK(cudaGetLastError());
+    dots_finish(g, p.nblk, k, out, 2, s);
 }
 
 void col_norms(bie_geom* g, const double* X, int k, double* out, cudaStream_t s) {
@@ -485,33 +502,25 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             double* Vj = V + (size_t)j * nk;
             apply_op(g, Vj, W, k, prec, flags, pre, s);
             ++res.matvecs;
-            // classical Gram-Schmidt, twice
+            // classical Gram-Schmidt, twice; the second pass is fused with the norm of the
+            // new direction and its coefficients are added to the first pass's in the Givens step
             dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
             {
                 Prof pf(g, BIE_KERNEL_KRYLOV, s);
                 k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
             }
             dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
-            {
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h2.as<double>(), n, k);
-            }
-            {
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_axpby<<<grid1((j + 1) * k), 256, 0, s>>>(1.0, g->h2.as<double>(), 1.0, g->h.as<double>(), j + 1, k,
-                nullptr);
-            }
-            col_norms(g, W, k, g->hn.as<double>(), s);
+            gs_update_norm(g, W, V, nk, j + 1, g->h2.as<double>(), k, g->hn.as<double>(), s);
             {
                 Prof pf(g, BIE_KERNEL_KRYLOV, s);
                 k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
             }
             {
                 Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->hn.as<double>(),
-                g->cs.as<double>(), g->sn.as<double>(), g->gv.as<double>(),
-                g->active.as<int>(), g->jlast.as<int>(), g->eps.as<double>(),
-                g->resid.as<double>(), j, m1, k);
+                k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->h2.as<double>(),
+                                                    g->hn.as<double>(), g->cs.as<double>(), g->sn.as<double>(),
+                                                    g->gv.as<double>(), g->active.as<int>(), g->jlast.as<int>(),
+                                                    g->eps.as<double>(), g->resid.as<double>(), j, m1, k);
             }
             BIE_CK(cudaGetLastError());
             ++it;
