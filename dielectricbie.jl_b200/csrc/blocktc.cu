@@ -17,7 +17,7 @@
 // tensor-core accumulation error grows with the number of accumulation steps;
 // restarting it every period bounds it by that of 256 sources, and the running
 // sum of the periods (round-to-nearest additions) adds a random-walk error of a
-// few units in the last place. Each source split writes the sum as an FP64 partial.
+// few units in the last place. Each source split writes the sum as an FP32 partial.
 //
 // CTA = 128 NQ + 64 threads: warps 0 .. 4 NQ - 1 generate the 128 x 64 kernel tile
 // of a source chunk (NQ threads per target row, each writing 64 / NQ of the row's
@@ -71,7 +71,7 @@ struct Params {
     int64_t nchunks;
     int64_t cps;           // chunks per split
     int sa, sb;            // A and B ring stages (2 .. SAMAX, 2 .. SBMAX)
-    double* part;          // [nsplit][n][ldp]
+    float* part;           // [nsplit][n][ldp] FP32 split partials
     int ldp, c0;
     int* err;
 };
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
         ok = !gen_any<NGEN>(!ok);  // every generator warp takes the same branch
         if (ok) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            double* out = P.part + ((int64_t)blockIdx.y * n + i) * P.ldp + P.c0;
+            float* out = P.part + ((int64_t)blockIdx.y * n + i) * P.ldp + P.c0;
             for (int c = qt * 16; c < npad; c += 16 * NQ) {
                 float h[16];
                 if (nch > 0) {
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
                 if (valid) {
 #pragma unroll
                     for (int q = 0; q < 16; ++q)
-                        if (c + q < P.keff) out[c + q] = (double)sgn * (double)h[q];
+                        if (c + q < P.keff) out[c + q] = sgn * h[q];
                 }
             }
         }
@@ -714,7 +714,7 @@ void launch_k(const Params& P, dim3 grid, size_t sm, cudaStream_t s) {
 
 template <int NP>
 void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit, int64_t cps,
-               double* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s) {
+               float* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s) {
     const int npad = ((kc + 15) / 16) * 16;
     const int64_t nchunks = (g.n + KC - 1) / KC;
     const int64_t pk = nchunks * npad * 8;
@@ -749,7 +749,7 @@ int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
 // with the kernel and right-hand sides split into `pieces` (2: three products,
 // 3: six products) bf16 pieces.
 void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
-                     int64_t cps, double* part, int ldp, uint8_t* bpack, int* err, int pieces, cudaStream_t s) {
+                     int64_t cps, float* part, int ldp, uint8_t* bpack, int* err, int pieces, cudaStream_t s) {
     if (pieces == 3)
         tc::launch_tc<3>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, s);
     else

@@ -223,7 +223,8 @@ __global__ void k_reduce_parts(const double* __restrict__ part, int nsplit, int6
 // of mul!(Y, ::BatchedDielectricOperator, X) (src/solver/multi_rhs.jl:120-128).
 // One thread per output; threads of a warp cover consecutive (i, c).
 // ---------------------------------------------------------------------------
-__global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int nsplit,
+template <typename TP>
+__global__ void k_combine(int64_t n, int k, const TP* __restrict__ part, int nsplit,
                           const double* __restrict__ X, int ldx, const double* __restrict__ pre,
                           const double* __restrict__ diag, const int32_t* __restrict__ rowptr,
                           const int32_t* __restrict__ col, const double* __restrict__ val, int nb,
@@ -234,7 +235,7 @@ __global__ void k_combine(int64_t n, int k, const double* __restrict__ part, int
     int c = (int)(e - i * k);
     double s = 0.0;
     const int64_t tot = n * (int64_t)k;
-    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * tot + e];
+    for (int p = 0; p < nsplit; ++p) s += (double)part[(int64_t)p * tot + e];
     s *= kInv4Pi;
     if (val) {
         int64_t P = i / nb;
@@ -302,8 +303,8 @@ inline size_t combine_smem_bytes(int nb) {
     return sizeof(double) * (2 * (size_t)kp * ldc + 2 * (size_t)kp * kCombLDX + 2 * (size_t)kp);
 }
 
-template <int MT>
-__global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const double* __restrict__ part, int nsplit,
+template <int MT, typename TP>
+__global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP* __restrict__ part, int nsplit,
                                                       const double* __restrict__ X, const double* __restrict__ pre,
                                                       const double* __restrict__ diag,
                                                       const int32_t* __restrict__ rowptr,
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const do
             if (c >= c0 + kt) continue;
             const int64_t e = i * k + c;
             double sp = 0.0;
-            for (int p = 0; p < nsplit; ++p) sp += part[(int64_t)p * tot + e];
+            for (int p = 0; p < nsplit; ++p) sp += (double)part[(int64_t)p * tot + e];
             double y = sp * kInv4Pi + acc[m][h];
             if (diag) y += dgi * X[e];
             Y[e] = y;

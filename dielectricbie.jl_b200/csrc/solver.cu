@@ -263,7 +263,7 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
 // K3 launch plan: the number of source splits ns (<= 16, and at most 1024 chunks
 // per split) that minimises the time of the wave-quantised grid, which is
 // proportional to ceil(tiles ns / slots) / ns; ties go to fewer splits (each
-// split adds an FP64 partial for the combine to read).
+// split adds an FP32 partial for the combine to read).
 Split tc_split(const bie_geom* g, int kc, int pieces) {
     const int64_t tiles = (g->n + kTcTileM - 1) / kTcTileM;
     const int64_t chunks = (g->n + kTcChunk - 1) / kTcChunk;
@@ -290,34 +290,22 @@ Split tc_split(const bie_geom* g, int kc, int pieces) {
 Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, int pieces, cudaStream_t s) {
     GeomDev gd = gdev(g);
     Split sp = tc_split(g, std::min(k, 128), pieces);
-    g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
+    g->part.ensure(sizeof(float) * (size_t)sp.nsplit * g->n * k);
     g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 128), pieces));
     for (int c0 = 0; c0 < k; c0 += 128) {
         int kc = std::min(128, k - c0);
         const double npairs = (double)g->n * (g->n - 1);
         Prof pf(g, BIE_KERNEL_DIRECT_TC, s, 2, npairs, npairs * tc_npad(kc));
-        launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, g->bpack.as<uint8_t>(),
+        launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<float>(), k, g->bpack.as<uint8_t>(),
                         g->errflag.as<int>(), pieces, s);
     }
     return sp;
 }
 
-// Y = A(prec) (p .* X), node-major n x k (ldx = ldy = k).
-void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
-              cudaStream_t s) {
-    Split sp;
-    if ((prec == BIE_BF16X3 || prec == BIE_BF16X6) && k >= 16) {
-        sp = direct_sum_tc(g, X, k, pre, prec == BIE_BF16X6 ? 3 : 2, s);
-    } else {
-        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // tensor-core precisions with k < 16 run FP32
-        sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
-    }
-    const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
-    const bool dg = !(flags & BIE_NO_DIAG);
-    const double cbytes = (corr ? (double)g->nblocks * g->nb * g->nb * 8 + g->nblocks * 4.0 + (g->npanels + 1) * 4.0
-                                : 0.0) +
-                          (double)g->n * k * 8 * (2 + sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
-    Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
+// K4 launch for split partials of type TP (FP64 from K1/K2, FP32 from K3).
+template <typename TP>
+void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y, int k, const double* pre, bool corr,
+             bool dg, cudaStream_t s) {
     const double* dgp = dg ? g->diag.as<double>() : nullptr;
     const int32_t* rp = corr ? g->rowptr.as<int32_t>() : nullptr;
     const int32_t* cl = corr ? g->col.as<int32_t>() : nullptr;
@@ -327,18 +315,17 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
         const size_t sm = combine_smem_bytes(g->nb);
         static bool attr = false;
         if (!attr) {
-            const void* fs[] = {(const void*)k_combine_dmma<1>, (const void*)k_combine_dmma<2>,
-                                (const void*)k_combine_dmma<3>, (const void*)k_combine_dmma<4>,
-                                (const void*)k_combine_dmma<5>, (const void*)k_combine_dmma<6>,
-                                (const void*)k_combine_dmma<7>, (const void*)k_combine_dmma<8>};
+            const void* fs[] = {(const void*)k_combine_dmma<1, TP>, (const void*)k_combine_dmma<2, TP>,
+                                (const void*)k_combine_dmma<3, TP>, (const void*)k_combine_dmma<4, TP>,
+                                (const void*)k_combine_dmma<5, TP>, (const void*)k_combine_dmma<6, TP>,
+                                (const void*)k_combine_dmma<7, TP>, (const void*)k_combine_dmma<8, TP>};
             for (const void* f : fs)
                 BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
             attr = true;
         }
         dim3 grid((unsigned)g->npanels, (unsigned)((k + kCombTile - 1) / kCombTile));
-#define BIE_COMB(MT)                                                                                            \
-    k_combine_dmma<MT><<<grid, 128, sm, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, pre, dgp, rp, cl, vl, \
-                                             g->nb, Y)
+#define BIE_COMB(MT) \
+    k_combine_dmma<MT, TP><<<grid, 128, sm, s>>>(g->n, k, part, nsplit, X, pre, dgp, rp, cl, vl, g->nb, Y)
         switch (mt) {
             case 1: BIE_COMB(1); break;
             case 2: BIE_COMB(2); break;
@@ -351,10 +338,33 @@ void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t
         }
 #undef BIE_COMB
     } else {
-        k_combine<<<grid1(g->n * k), 256, 0, s>>>(g->n, k, g->part.as<double>(), sp.nsplit, X, k, pre, dgp, rp, cl,
-                                                  vl, g->nb, Y, k);
+        k_combine<TP><<<grid1(g->n * k), 256, 0, s>>>(g->n, k, part, nsplit, X, k, pre, dgp, rp, cl, vl, g->nb, Y, k);
     }
     BIE_CK(cudaGetLastError());
+}
+
+// Y = A(prec) (p .* X), node-major n x k (ldx = ldy = k).
+void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
+              cudaStream_t s) {
+    Split sp;
+    const bool tc = (prec == BIE_BF16X3 || prec == BIE_BF16X6) && k >= 16;
+    if (tc) {
+        sp = direct_sum_tc(g, X, k, pre, prec == BIE_BF16X6 ? 3 : 2, s);
+    } else {
+        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // tensor-core precisions with k < 16 run FP32
+        sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
+    }
+    const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
+    const bool dg = !(flags & BIE_NO_DIAG);
+    const double pbytes = tc ? 4.0 : 8.0;
+    const double cbytes = (corr ? (double)g->nblocks * g->nb * g->nb * 8 + g->nblocks * 4.0 + (g->npanels + 1) * 4.0
+                                : 0.0) +
+                          (double)g->n * k * (16.0 + pbytes * sp.nsplit) + (dg ? g->n * 8.0 : 0.0);
+    Prof pf(g, BIE_KERNEL_COMBINE, s, 1, 0, 0, cbytes);
+    if (tc)
+        combine(g, g->part.as<float>(), sp.nsplit, X, Y, k, pre, corr, dg, s);
+    else
+        combine(g, g->part.as<double>(), sp.nsplit, X, Y, k, pre, corr, dg, s);
 }
 
 // ------------------------------ reductions ---------------------------------
