@@ -197,6 +197,17 @@ def run_reference_arm(args, wl):
     return 0
 
 
+def profiled_traffic(name):
+    """DRAM bytes (read + written) per launch of a kernel, from the ncu summary
+    committed under profiles/ (its `dram_bytes_per_launch:` line); None if absent."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    import re
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
 def workload_config(name, wl, n):
     return {"workload": f"{name}: block {wl['k']}-RHS solve, box {'x'.join(str(v) for v in wl['box'])}, "
                         f"n_quad={wl['nq']}, l_ec={wl['l_ec']}, eps {wl['eps_in']}/{wl['eps_out']}, N={n}",
@@ -283,7 +294,7 @@ def main():
         if rc != _abi.BIE_OK:
             _abi.check(rc)
 
-    def timed_loop(precision, rtol, profile=False, sampler_dev=None):
+    def timed_loop(precision, rtol, tag, profile=False):
         ms = []
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for i in range(nsteps):
@@ -291,11 +302,15 @@ def main():
             torch.cuda.synchronize(device)
             if i == args.warmup and profile:
                 _abi.check(L.bie_profile_enable(g, 1))
+            if i >= args.warmup:  # NVTX range of a timed step (ncu --nvtx-include "<tag>_step/")
+                torch.cuda.nvtx.range_push(f"{tag}_step")
             with torch.cuda.stream(stream):
                 ev0.record(stream)
                 solve_step(i, precision, rtol)
                 ev1.record(stream)
             ev1.synchronize()
+            if i >= args.warmup:
+                torch.cuda.nvtx.range_pop()
             if i >= args.warmup:
                 ms.append(ev0.elapsed_time(ev1))
         return ms
@@ -335,14 +350,14 @@ def main():
     if dist is not None:
         dist.barrier()
     with ClockSampler(device) as clk:
-        ms_ref = timed_loop(args.precision, wl["rtol"], profile=True)
+        ms_ref = timed_loop(args.precision, wl["rtol"], "refined", profile=True)
     kt = {}
     for name, kind in _abi.KERNEL_KINDS.items():
         t = _abi.KernelTime()
         _abi.check(L.bie_profile_read(g, kind, C.byref(t)))
         kt[name] = t
     _abi.check(L.bie_profile_enable(g, 0))
-    ms_plain = timed_loop("fp64", wl["rtol"])
+    ms_plain = timed_loop("fp64", wl["rtol"], "plain")
 
     total_ms = float(np.sum(ms_ref))
     total_plain = float(np.sum(ms_plain))
@@ -401,7 +416,9 @@ def main():
         achieved = flops / (per_launch_ms * 1e-3) / 1e12
         roofline = {"kernel": "k_dt_tc (tcgen05 split-BF16 x3 block direct sum, incl. Q packing)", "bound": "tensor",
                     "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
-                    "peak_source": f"bf16_tflops_sustained {peak_src}", "traffic": None,
+                    "peak_source": f"bf16_tflops_sustained {peak_src}",
+                    "traffic": profiled_traffic(f"k_dt_tc_{args.workload}.md"),
+                    "traffic_source": f"profiles/k_dt_tc_{args.workload}.md (ncu dram bytes read + written per launch)",
                     "per_launch_ms": per_launch_ms}
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         fp32_issue_peak = 148 * 128 * sm_mhz * 1e6  # FP32 lane-instructions/s at the sampled clock
