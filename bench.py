@@ -197,6 +197,23 @@ def run_reference_arm(args, wl):
     return 0
 
 
+def max_over_ranks(dist, values, device=None):
+    """Element-wise maximum of per-rank timings over the process group (the
+    slowest replica sets the job's time). Device tensors for NCCL, host tensors
+    for gloo."""
+    import torch
+    on_dev = dist.get_backend() == "nccl"
+    t = torch.tensor(values, dtype=torch.float64, device=(f"cuda:{device}" if on_dev else "cpu"))
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def replica_value(per_rank_units, world, time_ms):
+    """Whole-job throughput of independent replicas: all ranks' units over the
+    slowest rank's time."""
+    return per_rank_units * world / (time_ms * 1e-3)
+
+
 def profiled_traffic(name):
     """DRAM bytes (read + written) per launch of a kernel, from the ncu summary
     committed under profiles/ (its `dram_bytes_per_launch:` line); None if absent."""
@@ -362,12 +379,10 @@ def main():
     total_ms = float(np.sum(ms_ref))
     total_plain = float(np.sum(ms_plain))
     if dist is not None:
-        tt = torch.tensor([total_ms, total_plain], dtype=torch.float64, device=device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms, total_plain = float(tt[0]), float(tt[1])
+        total_ms, total_plain = max_over_ranks(dist, [total_ms, total_plain], device)
     solves = k * args.steps * world
-    value = solves / (total_ms * 1e-3)
-    plain_value = solves / (total_plain * 1e-3)
+    value = replica_value(k * args.steps, world, total_ms)
+    plain_value = replica_value(k * args.steps, world, total_plain)
 
     # ---------------- e2e: reference-shaped host API with host buffers ---------------
     pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
@@ -391,9 +406,7 @@ def main():
             e2e_ms.append((t1 - t0) * 1e3)
     e2e_total = float(np.sum(e2e_ms))
     if dist is not None:
-        tt = torch.tensor([e2e_total], dtype=torch.float64, device=device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt[0])
+        (e2e_total,) = max_over_ranks(dist, [e2e_total], device)
     e2e_value = solves / (e2e_total * 1e-3)
 
     # ---------------- roofline of the dominant kernel ------------------------------
