@@ -519,12 +519,7 @@ class SolveStats:
     col_resid: np.ndarray
 
 
-def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float = 0.0, itmax: int = 500,
-              restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
-              precondition: bool = False, check_every: int = 1, raise_on_noconv: bool = False):
-    """Solve A Sigma = F on the device. Returns (Sigma, SolveStats)."""
-    Ff, vec = _as_cols(F, op.n)
-    k = Ff.shape[1]
+def _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every):
     o = _abi.SolveOpts()
     lib().bie_solve_opts_default(C.byref(o))
     o.atol, o.rtol, o.itmax, o.restart = float(atol), float(rtol), int(itmax), int(restart)
@@ -532,6 +527,16 @@ def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float 
     o.inner_rtol, o.max_outer, o.precondition, o.check_every = float(inner_rtol), int(max_outer), int(precondition), int(check_every)
     if op.near is None:
         o.flags = 0
+    return o
+
+
+def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float = 0.0, itmax: int = 500,
+              restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
+              precondition: bool = False, check_every: int = 1, raise_on_noconv: bool = False):
+    """Solve A Sigma = F on the device. Returns (Sigma, SolveStats)."""
+    Ff, vec = _as_cols(F, op.n)
+    k = Ff.shape[1]
+    o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
     ci = np.zeros(k, dtype=np.intc)
     cr = np.zeros(k)
     st = _abi.Stats()
@@ -544,6 +549,85 @@ def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float 
     stats = SolveStats(st.iterations, st.outer, st.fp64_matvecs, st.lowp_matvecs, bool(st.converged),
                        st.max_rel_resid, st.seconds, ci.copy(), cr.copy())
     return (S[:, 0] if vec else S), stats
+
+
+class SolveServer:
+    """Request server with continuous batching (C-ABI ``bie_server_*``).
+
+    ``submit(op, F, ...)`` queues a block solve of F (N x k) on the operator's
+    device-resident geometry and returns a ticket; ``result(ticket)`` waits for it and
+    returns (Sigma, SolveStats, latency_ms). Up to ``max_slots`` block solves run at
+    once, each on its geometry's stream; queued requests for the same geometry and
+    options are merged into one block solve of at most ``max_batch_rhs`` columns;
+    admission also respects an HBM budget (``hbm_fraction`` of the free memory).
+    An operator handed to a server must not be used directly until its requests
+    have been collected."""
+
+    def __init__(self, *, max_slots: int = 4, max_batch_rhs: int = 64, hbm_fraction: float = 0.8, device: int = 0):
+        o = _abi.ServerOpts()
+        lib().bie_server_opts_default(C.byref(o))
+        o.max_slots, o.max_batch_rhs, o.hbm_fraction, o.device = int(max_slots), int(max_batch_rhs), \
+            float(hbm_fraction), int(device)
+        h = C.c_void_p()
+        check(lib().bie_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._shapes = {}
+
+    def submit(self, op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float = 0.0, itmax: int = 500,
+               restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
+               precondition: bool = False, check_every: int = 1) -> int:
+        Ff, vec = _as_cols(F, op.n)
+        k = Ff.shape[1]
+        o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+        t = C.c_uint64(0)
+        check(lib().bie_server_submit(self._h, op.geom._h, dptr(Ff), k, C.byref(o), C.byref(t)))
+        self._shapes[t.value] = (op.n, k, vec)
+        return t.value
+
+    def result(self, ticket: int, timeout_ms: int = -1):
+        """(Sigma, SolveStats, latency_ms) once the request finished, else None after timeout_ms."""
+        n, k, vec = self._shapes[ticket]
+        S = np.zeros((n, k), order="F")
+        ci = np.zeros(k, dtype=np.intc)
+        cr = np.zeros(k)
+        st = _abi.Stats()
+        st.col_iterations = ci.ctypes.data_as(C.POINTER(C.c_int))
+        st.col_resid = cr.ctypes.data_as(C.POINTER(C.c_double))
+        lat = C.c_double(0.0)
+        done = C.c_int(0)
+        rc = lib().bie_server_poll(self._h, ticket, int(timeout_ms), dptr(S), C.byref(st), C.byref(lat),
+                                   C.byref(done))
+        if rc not in (_abi.BIE_OK, _abi.BIE_ENOCONV):
+            del self._shapes[ticket]
+            check(rc)
+        if not done.value:
+            return None
+        del self._shapes[ticket]
+        stats = SolveStats(st.iterations, st.outer, st.fp64_matvecs, st.lowp_matvecs, rc == _abi.BIE_OK,
+                           st.max_rel_resid, st.seconds, ci, cr)
+        return (S[:, 0] if vec else S), stats, lat.value
+
+    def counters(self) -> dict:
+        c = _abi.ServerCounters()
+        check(lib().bie_server_counters_read(self._h, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def close(self):
+        if self._h:
+            lib().bie_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def solve_gmres(A: GPUDielectricOperator, b, atol: float = 1e-6, rtol: float = 1e-6, itmax: int = 1000):

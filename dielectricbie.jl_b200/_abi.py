@@ -27,6 +27,8 @@ EXPORTS = [
     "bie_geom_destroy", "bie_matvec", "bie_matvec_device", "bie_rhs_point", "bie_rhs_point_device",
     "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve",
     "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
+    "bie_server_opts_default", "bie_server_create", "bie_server_submit", "bie_server_poll",
+    "bie_server_counters_read", "bie_server_destroy",
 ]
 
 
@@ -50,6 +52,18 @@ class SolveOpts(C.Structure):
     _fields_ = [("atol", C.c_double), ("rtol", C.c_double), ("itmax", C.c_int), ("restart", C.c_int),
                 ("precision", C.c_int), ("inner_rtol", C.c_double), ("max_outer", C.c_int),
                 ("precondition", C.c_int), ("check_every", C.c_int), ("flags", C.c_uint32)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("max_slots", C.c_int), ("max_batch_rhs", C.c_int), ("hbm_fraction", C.c_double),
+                ("device", C.c_int)]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("batches", C.c_int64),
+                ("merged_requests", C.c_int64), ("queued", C.c_int64), ("inflight", C.c_int),
+                ("peak_inflight", C.c_int), ("hbm_budget", C.c_int64), ("hbm_in_use", C.c_int64),
+                ("hbm_peak", C.c_int64)]
 
 
 class KernelTime(C.Structure):
@@ -118,6 +132,13 @@ def lib():
         "bie_profile_enable": (i, [_vp, i]),
         "bie_profile_read": (i, [_vp, i, C.POINTER(KernelTime)]),
         "bie_dt_apply_static": (i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, i64, _vp, C.c_int32, _vp, _vp]),
+        "bie_server_opts_default": (None, [C.POINTER(ServerOpts)]),
+        "bie_server_create": (i, [C.POINTER(ServerOpts), C.POINTER(_vp)]),
+        "bie_server_submit": (i, [_vp, _vp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(C.c_uint64)]),
+        "bie_server_poll": (i, [_vp, C.c_uint64, C.c_int32, _dp, C.POINTER(Stats), C.POINTER(C.c_double),
+                                C.POINTER(C.c_int)]),
+        "bie_server_counters_read": (i, [_vp, C.POINTER(ServerCounters)]),
+        "bie_server_destroy": (None, [_vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -25,6 +28,45 @@ thread_local std::string g_last_error;
 
 void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(BIE_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+std::mutex g_attr_mu;
+std::map<std::pair<int, const void*>, size_t> g_smem_limit;
+std::map<std::tuple<int, const void*, int, size_t>, int> g_occ;
+int current_device() {
+    int d = 0;
+    cuda_check(cudaGetDevice(&d), "cudaGetDevice");
+    return d;
+}
+}  // namespace
+
+void ensure_smem_limit(const void* f, size_t bytes) {
+    if (bytes <= 48 * 1024) return;
+    const int dev = current_device();
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    size_t& cur = g_smem_limit[{dev, f}];
+    if (bytes <= cur) return;
+    cuda_check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+               "cudaFuncSetAttribute");
+    cur = bytes;
+}
+
+int occupancy(const void* f, int threads, size_t smem) {
+    const int dev = current_device();
+    {
+        std::lock_guard<std::mutex> lock(g_attr_mu);
+        auto it = g_occ.find({dev, f, threads, smem});
+        if (it != g_occ.end()) return it->second;
+    }
+    ensure_smem_limit(f, smem);
+    int occ = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, threads, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    occ = std::max(occ, 1);
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    g_occ[{dev, f, threads, smem}] = occ;
+    return occ;
 }
 
 void Buf::ensure(size_t need) {
@@ -311,6 +353,56 @@ int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int3
         REQUIRE(g && dX && dY && k >= 1, "matvec_device: bad argument");
         bie::matvec_device(g, dX, dY, k, precision, flags, (cudaStream_t)stream);
     });
+}
+
+void bie_server_opts_default(bie_server_opts* o) {
+    if (!o) return;
+    o->max_slots = 4;
+    o->max_batch_rhs = 64;
+    o->hbm_fraction = 0.8;
+    o->device = 0;
+}
+
+int bie_server_create(const bie_server_opts* o, bie_server** out) {
+    return guarded([&] {
+        REQUIRE(out, "server_create: bad argument");
+        bie_server_opts d;
+        bie_server_opts_default(&d);
+        *out = bie::server_create(o ? *o : d);
+    });
+}
+
+int bie_server_submit(bie_server* s, bie_geom* g, const double* F, int32_t k, const bie_solve_opts* o,
+                      uint64_t* ticket) {
+    return guarded([&] {
+        REQUIRE(s && g && F && ticket && k >= 1, "server_submit: bad argument");
+        bie_solve_opts d;
+        bie_solve_opts_default(&d);
+        *ticket = bie::server_submit(s, g, F, k, o ? *o : d);
+    });
+}
+
+int bie_server_poll(bie_server* s, uint64_t ticket, int32_t timeout_ms, double* Sigma, bie_stats* st,
+                    double* latency_ms, int* done) {
+    int rc = BIE_OK;
+    const int g = guarded([&] {
+        REQUIRE(s && done, "server_poll: bad argument");
+        std::string err;
+        rc = bie::server_poll(s, ticket, timeout_ms, Sigma, st, latency_ms, done, &err);
+        if (rc != BIE_OK) bie::g_last_error = err;
+    });
+    return g != BIE_OK ? g : rc;
+}
+
+int bie_server_counters_read(bie_server* s, bie_server_counters* out) {
+    return guarded([&] {
+        REQUIRE(s && out, "server_counters: bad argument");
+        bie::server_counters(s, out);
+    });
+}
+
+void bie_server_destroy(bie_server* s) {
+    if (s) bie::server_destroy(s);
 }
 
 int bie_dt_apply_static(const double* x, const double* y, const double* z, const double* nx, const double* ny,

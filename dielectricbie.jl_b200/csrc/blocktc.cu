@@ -703,11 +703,7 @@ Shape shape(int npad, int np) {
 
 template <int NP, int NQ>
 void launch_k(const Params& P, dim3 grid, size_t sm, cudaStream_t s) {
-    static size_t configured = 0;
-    if (sm > configured) {
-        BIE_CK(cudaFuncSetAttribute(k_dt_tc<NP, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        configured = sm;
-    }
+    ensure_smem_limit((const void*)k_dt_tc<NP, NQ>, sm);
     k_dt_tc<NP, NQ><<<grid, nthreads<NQ>(), sm, s>>>(P);
     BIE_CK(cudaGetLastError());
 }

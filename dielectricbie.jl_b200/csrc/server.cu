@@ -1,0 +1,307 @@
+// Request server: the serving loop around the block solve
+// (solve_dielectric_box3d_block, src/solver/multi_rhs.jl:270-286).
+//
+// Requests (a geometry handle, an N x k block of right-hand sides, solver
+// options) are queued by bie_server_submit. A fixed number of worker threads
+// ("slots") take admissible work from the queue: the oldest request whose
+// geometry is not already being solved and whose estimated device workspace fits
+// the HBM budget, merged with every later queued request for the same geometry
+// and options up to max_batch_rhs columns — one block solve, one set of direct-sum
+// launches for all of them. Batches on different geometries run at the same time,
+// each on its geometry's CUDA stream, so their kernels overlap on the GPU; work
+// that arrives while others run is admitted as slots and budget free up
+// (continuous batching). Every column of a block solve runs its own Krylov process,
+// so a request's result does not depend on what it was batched with beyond
+// floating-point rounding.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "solver.h"
+
+namespace bie {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t ticket = 0;
+    bie_geom* g = nullptr;
+    int64_t n = 0;
+    int k = 0;
+    bie_solve_opts o{};
+    std::vector<double> F, S;  // N x k column-major
+    std::vector<int> col_it;
+    std::vector<double> col_res;
+    bie_stats st{};
+    int rc = BIE_OK;
+    std::string err;
+    bool done = false;
+    Clock::time_point t_submit, t_start, t_done;
+};
+
+bool same_opts(const bie_solve_opts& a, const bie_solve_opts& b) {
+    return a.atol == b.atol && a.rtol == b.rtol && a.itmax == b.itmax && a.restart == b.restart &&
+           a.precision == b.precision && a.inner_rtol == b.inner_rtol && a.max_outer == b.max_outer &&
+           a.precondition == b.precondition && a.check_every == b.check_every && a.flags == b.flags;
+}
+
+// Device workspace of a block solve of k columns: the Krylov basis (restart + 1
+// vectors) plus about 32 more N x k blocks (residuals, split partials, I/O).
+size_t footprint(int64_t n, int k, const bie_solve_opts& o) {
+    const int64_t m = std::max(1, std::min(o.restart, o.itmax));
+    return (size_t)(m + 1 + 32) * (size_t)n * (size_t)k * sizeof(double);
+}
+
+}  // namespace
+}  // namespace bie
+
+struct bie_server {
+    bie_server_opts opt{};
+    size_t budget = 0, in_use = 0, peak_use = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<bie::Request>> queue;
+    std::unordered_map<uint64_t, std::shared_ptr<bie::Request>> table;
+    std::unordered_map<bie_geom*, int> busy;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    int inflight = 0;
+    bie_server_counters cnt{};
+    std::vector<std::thread> workers;
+};
+
+namespace bie {
+namespace {
+
+// Takes the next admissible batch off the queue (caller holds s->mu).
+bool take_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch, size_t& fp) {
+    for (size_t i = 0; i < s->queue.size(); ++i) {
+        const std::shared_ptr<Request> r = s->queue[i];
+        if (s->busy.count(r->g)) continue;
+        // gather the oldest request and later ones it can be merged with
+        std::vector<size_t> pick{i};
+        int K = r->k;
+        for (size_t j = i + 1; j < s->queue.size(); ++j) {
+            const auto& q = s->queue[j];
+            if (q->g == r->g && same_opts(q->o, r->o) && K + q->k <= s->opt.max_batch_rhs) {
+                pick.push_back(j);
+                K += q->k;
+            }
+        }
+        const size_t need = footprint(r->n, K, r->o);
+        if (s->inflight > 0 && s->in_use + need > s->budget) continue;  // admitted later, when memory frees
+        batch.clear();
+        for (size_t j : pick) batch.push_back(s->queue[j]);
+        for (size_t t = pick.size(); t-- > 0;) s->queue.erase(s->queue.begin() + (std::ptrdiff_t)pick[t]);
+        s->busy[r->g] = 1;
+        s->in_use += need;
+        s->peak_use = std::max(s->peak_use, s->in_use);
+        fp = need;
+        return true;
+    }
+    return false;
+}
+
+void run_batch(std::vector<std::shared_ptr<Request>>& batch) {
+    const auto& r0 = batch.front();
+    const int64_t n = r0->n;
+    int K = 0;
+    for (auto& r : batch) K += r->k;
+    std::vector<double> F((size_t)n * K), S((size_t)n * K);
+    std::vector<int> col_it(K, 0);
+    std::vector<double> col_res(K, 0.0);
+    int off = 0;
+    for (auto& r : batch) {
+        std::memcpy(F.data() + (size_t)off * n, r->F.data(), sizeof(double) * (size_t)n * r->k);
+        off += r->k;
+    }
+    bie_stats st{};
+    st.col_iterations = col_it.data();
+    st.col_resid = col_res.data();
+    int rc = BIE_OK;
+    std::string err;
+    const auto t_start = Clock::now();
+    try {
+        rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+        if (rc != BIE_OK) err = "solver did not converge to the requested tolerance";
+    } catch (const Error& e) {
+        rc = e.code;
+        err = e.what();
+    } catch (const std::exception& e) {
+        rc = BIE_EINVAL;
+        err = e.what();
+    }
+    off = 0;
+    for (auto& r : batch) {
+        r->t_start = t_start;
+        if (rc == BIE_OK || rc == BIE_ENOCONV) {
+            r->S.assign(S.begin() + (size_t)off * n, S.begin() + (size_t)(off + r->k) * n);
+            r->col_it.assign(col_it.begin() + off, col_it.begin() + off + r->k);
+            r->col_res.assign(col_res.begin() + off, col_res.begin() + off + r->k);
+        }
+        r->st = st;
+        r->st.col_iterations = nullptr;
+        r->st.col_resid = nullptr;
+        double mx = 0.0;
+        for (double v : r->col_res) mx = std::max(mx, v);
+        r->st.max_rel_resid = mx;
+        r->rc = rc;
+        r->err = err;
+        off += r->k;
+    }
+}
+
+void worker(bie_server* s) {
+    for (;;) {
+        std::vector<std::shared_ptr<Request>> batch;
+        size_t fp = 0;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            for (;;) {
+                if (s->stop) return;
+                if (take_batch(s, batch, fp)) break;
+                s->cv_work.wait(lk);
+            }
+            ++s->inflight;
+            s->cnt.batches += 1;
+            s->cnt.merged_requests += (int64_t)batch.size() - 1;
+            s->cnt.peak_inflight = std::max(s->cnt.peak_inflight, s->inflight);
+        }
+        run_batch(batch);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            const auto now = Clock::now();
+            for (auto& r : batch) {
+                r->t_done = now;
+                r->done = true;
+            }
+            s->busy.erase(batch.front()->g);
+            s->in_use -= fp;
+            --s->inflight;
+            s->cnt.completed += (int64_t)batch.size();
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+}
+
+}  // namespace
+
+bie_server* server_create(const bie_server_opts& o) {
+    if (o.max_slots < 1 || o.max_slots > 64 || o.max_batch_rhs < 1 || o.max_batch_rhs > 256 ||
+        !(o.hbm_fraction > 0.0 && o.hbm_fraction <= 1.0))
+        throw Error(BIE_EINVAL, "server_create: bad options");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        throw Error(BIE_ENODEVICE, "server_create: no CUDA device");
+    }
+    if (o.device < 0 || o.device >= ndev) throw Error(BIE_EINVAL, "server_create: bad device");
+    int prev = 0;
+    BIE_CK(cudaGetDevice(&prev));
+    BIE_CK(cudaSetDevice(o.device));
+    size_t free_b = 0, total_b = 0;
+    const cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+    cudaSetDevice(prev);
+    BIE_CK(e);
+    auto s = std::make_unique<bie_server>();
+    s->opt = o;
+    s->budget = (size_t)(o.hbm_fraction * (double)free_b);
+    s->cnt.hbm_budget = (int64_t)s->budget;
+    for (int i = 0; i < o.max_slots; ++i) s->workers.emplace_back(worker, s.get());
+    return s.release();
+}
+
+void server_destroy(bie_server* s) {
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->workers) t.join();
+    delete s;
+}
+
+uint64_t server_submit(bie_server* s, bie_geom* g, const double* F, int k, const bie_solve_opts& o) {
+    int64_t n = 0, nblocks = 0;
+    size_t bytes = 0;
+    geom_info(g, &n, &nblocks, &bytes);
+    if (k < 1 || k > s->opt.max_batch_rhs)
+        throw Error(BIE_EINVAL, "server_submit: k must be in [1, max_batch_rhs]");
+    auto r = std::make_shared<Request>();
+    r->g = g;
+    r->n = n;
+    r->k = k;
+    r->o = o;
+    r->F.assign(F, F + (size_t)n * k);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) throw Error(BIE_EINVAL, "server_submit: server is shutting down");
+        r->ticket = s->next_ticket++;
+        s->queue.push_back(r);
+        s->table[r->ticket] = r;
+        s->cnt.submitted += 1;
+    }
+    s->cv_work.notify_one();
+    return r->ticket;
+}
+
+int server_poll(bie_server* s, uint64_t ticket, int timeout_ms, double* Sigma, bie_stats* st, double* latency_ms,
+                int* done, std::string* err) {
+    std::shared_ptr<Request> r;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->table.find(ticket);
+        if (it == s->table.end()) throw Error(BIE_EINVAL, "server_poll: unknown ticket");
+        r = it->second;
+        auto ready = [&] { return r->done; };
+        if (timeout_ms < 0)
+            s->cv_done.wait(lk, ready);
+        else
+            s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
+        if (!r->done) {
+            *done = 0;
+            return BIE_OK;
+        }
+        s->table.erase(it);
+    }
+    *done = 1;
+    if (Sigma && !r->S.empty()) std::memcpy(Sigma, r->S.data(), sizeof(double) * r->S.size());
+    if (st) {
+        int* ci = st->col_iterations;
+        double* cr = st->col_resid;
+        *st = r->st;
+        st->col_iterations = ci;
+        st->col_resid = cr;
+        if (ci)
+            for (int c = 0; c < r->k && c < (int)r->col_it.size(); ++c) ci[c] = r->col_it[c];
+        if (cr)
+            for (int c = 0; c < r->k && c < (int)r->col_res.size(); ++c) cr[c] = r->col_res[c];
+    }
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    *err = r->err;
+    return r->rc;
+}
+
+void server_counters(bie_server* s, bie_server_counters* out) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->cnt;
+    out->queued = (int64_t)s->queue.size();
+    out->inflight = s->inflight;
+    out->hbm_in_use = (int64_t)s->in_use;
+    out->hbm_peak = (int64_t)s->peak_use;
+}
+
+}  // namespace bie

@@ -153,19 +153,10 @@ size_t kern_smem(Kern kind) {
     return (size_t)(3 + C) * kTS * (kind == Kern::DT32 ? sizeof(float) : sizeof(double));
 }
 
-// occupancy (CTAs per SM) of one instantiation; also raises the dynamic smem limit once
+// occupancy (CTAs per SM) of one instantiation; also raises its dynamic smem limit
 template <int C>
 int kern_occ(Kern kind) {
-    static int cache[3] = {0, 0, 0};
-    int idx = (int)kind;
-    if (cache[idx]) return cache[idx];
-    size_t sm = kern_smem<C>(kind);
-    void* f = kern_ptr<C>(kind);
-    if (sm > 48 * 1024) BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    int occ = 0;
-    BIE_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, kTB, sm));
-    cache[idx] = std::max(occ, 1);
-    return cache[idx];
+    return occupancy(kern_ptr<C>(kind), kTB, kern_smem<C>(kind));
 }
 
 struct Split {
@@ -313,18 +304,9 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
     const int mt = (g->nb + 7) / 8;
     if (g->nb > 0 && mt <= 8 && (int64_t)g->npanels * g->nb == g->n) {
         const size_t sm = combine_smem_bytes(g->nb);
-        static bool attr = false;
-        if (!attr) {
-            const void* fs[] = {(const void*)k_combine_dmma<1, TP>, (const void*)k_combine_dmma<2, TP>,
-                                (const void*)k_combine_dmma<3, TP>, (const void*)k_combine_dmma<4, TP>,
-                                (const void*)k_combine_dmma<5, TP>, (const void*)k_combine_dmma<6, TP>,
-                                (const void*)k_combine_dmma<7, TP>, (const void*)k_combine_dmma<8, TP>};
-            for (const void* f : fs)
-                BIE_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
-            attr = true;
-        }
         dim3 grid((unsigned)g->npanels, (unsigned)((k + kCombTile - 1) / kCombTile));
-#define BIE_COMB(MT) \
+#define BIE_COMB(MT)                                       \
+    ensure_smem_limit((const void*)k_combine_dmma<MT, TP>, sm); \
     k_combine_dmma<MT, TP><<<grid, 128, sm, s>>>(g->n, k, part, nsplit, X, pre, dgp, rp, cl, vl, g->nb, Y)
         switch (mt) {
             case 1: BIE_COMB(1); break;

@@ -18,6 +18,12 @@ struct Error : std::runtime_error {
 void cuda_check(cudaError_t e, const char* what);
 #define BIE_CK(call) ::bie::cuda_check((call), #call)
 
+// Raises the dynamic shared-memory limit of kernel f on the current device to at
+// least `bytes` (never lowers it). Thread-safe; the limit is kept per device.
+void ensure_smem_limit(const void* f, size_t bytes);
+// CTAs per SM of kernel f with `threads` threads and `smem` bytes, cached per device.
+int occupancy(const void* f, int threads, size_t smem);
+
 // Grow-only device buffer owned by a geometry handle.
 struct Buf {
     void* p = nullptr;
@@ -48,6 +54,14 @@ void energy_host(bie_geom* g, const double* S, int k, const double* src, const d
 int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_solve_opts& o, bie_stats* st);
 int solve_device(bie_geom* g, const double* dF, double* dSigma, int k, const bie_solve_opts& o, bie_stats* st,
                  cudaStream_t s);
+
+// server.cu: request server with continuous batching of block solves.
+bie_server* server_create(const bie_server_opts& o);
+void server_destroy(bie_server* s);
+uint64_t server_submit(bie_server* s, bie_geom* g, const double* F, int k, const bie_solve_opts& o);
+int server_poll(bie_server* s, uint64_t ticket, int timeout_ms, double* Sigma, bie_stats* st, double* latency_ms,
+                int* done, std::string* err);
+void server_counters(bie_server* s, bie_server_counters* out);
 
 // noalloc.cu: direct sum with the split partials in a fixed device array.
 int64_t dt_apply_static_max_nodes();

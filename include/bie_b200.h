@@ -257,6 +257,45 @@ int bie_profile_enable(bie_geom* g, int enable);
 /* Reads the accumulated figures of one kernel kind (synchronises the stream). */
 int bie_profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 
+/* ---- request server: the serving loop around the block solve -------------------
+ * Requests of solve_dielectric_box3d_block (src/solver/multi_rhs.jl:270-286) --
+ * a geometry handle, an N x k block of right-hand sides and solver options -- are
+ * queued and solved by max_slots worker threads with continuous batching: a slot
+ * takes the oldest request whose geometry is idle and whose device workspace fits
+ * the HBM budget, merged with later queued requests for the same geometry and
+ * options (up to max_batch_rhs columns) into one block solve; batches on different
+ * geometries run concurrently on their geometries' streams. A geometry handle given
+ * to a server must not be used by other calls until its requests are polled. */
+typedef struct bie_server bie_server;
+
+typedef struct {
+    int max_slots;       /* block solves in flight at once (default 4) */
+    int max_batch_rhs;   /* columns merged into one block solve (default 64, <= 256) */
+    double hbm_fraction; /* admission budget: this fraction of the device's free memory at creation (0.8) */
+    int device;          /* CUDA device of the budget (the geometries carry their own) */
+} bie_server_opts;
+
+typedef struct {
+    int64_t submitted, completed, batches, merged_requests, queued;
+    int inflight, peak_inflight;
+    int64_t hbm_budget, hbm_in_use, hbm_peak; /* bytes of estimated solver workspace */
+} bie_server_counters;
+
+void bie_server_opts_default(bie_server_opts* o);
+int bie_server_create(const bie_server_opts* o, bie_server** out);
+/* Copies F (host, N x k column-major) and queues the solve; *ticket identifies it. */
+int bie_server_submit(bie_server* s, bie_geom* g, const double* F, int32_t k, const bie_solve_opts* o,
+                      uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: until done) for the request. *done = 1 when finished:
+ * Sigma (host N x k, may be NULL), stats and the submit-to-completion latency are
+ * filled, the ticket is retired and the solve's status is returned (BIE_ENOCONV
+ * included); *done = 0 and BIE_OK while it is still queued or running. */
+int bie_server_poll(bie_server* s, uint64_t ticket, int32_t timeout_ms, double* Sigma, bie_stats* st,
+                    double* latency_ms, int* done);
+int bie_server_counters_read(bie_server* s, bie_server_counters* out);
+/* Stops the slots after their current batches; queued requests are dropped. */
+void bie_server_destroy(bie_server* s);
+
 #ifdef __cplusplus
 }
 #endif

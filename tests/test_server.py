@@ -1,0 +1,73 @@
+"""Request server (continuous batching): every request's sigma is the same solved
+alone and solved in a mix with other requests and geometries, within the refined
+parity bar (1e-8 relative per column); the mix really merges same-geometry
+requests into block solves and runs several geometries at once."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BOXES = [(1.2, 0.8, 0.6, 4, 0.2, 4.0, 1.0), (1.0, 0.6, 0.5, 4, 0.15, 10.0, 1.0), (0.8, 0.8, 0.8, 6, 0.25, 2.5, 1.0)]
+TOL = 1e-8
+
+
+def rel_cols(a, b):
+    return np.linalg.norm(a - b, axis=0) / np.linalg.norm(b, axis=0)
+
+
+@pytest.fixture(scope="module")
+def stream(bie):
+    rng = np.random.default_rng(2024)
+    ops = []
+    for b in BOXES:
+        itf = bie.single_dielectric_box3d(*b)
+        ops.append((itf, bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, 1e-9, 8), b))
+    reqs = []
+    for _ in range(14):
+        gi = int(rng.integers(len(ops)))
+        itf, op, b = ops[gi]
+        k = int(rng.integers(1, 21))
+        half = 0.4 * np.array(b[:3])
+        src = [bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal())) for _ in range(k)]
+        reqs.append((gi, bie.rhs_dielectric_box3d(itf, src, b[5])))
+    return ops, reqs
+
+
+def test_server_mix_equals_alone(bie, stream):
+    ops, reqs = stream
+    alone = [bie.gpu_solve(ops[gi][1], F, rtol=1e-10, precision="bf16x3")[0] for gi, F in reqs]
+    with bie.SolveServer(max_slots=3, max_batch_rhs=64) as srv:
+        tickets = [srv.submit(ops[gi][1], F, rtol=1e-10, precision="bf16x3") for gi, F in reqs]
+        out = [srv.result(t) for t in tickets]
+        cnt = srv.counters()
+    for (gi, F), ref, (S, st, lat) in zip(reqs, alone, out):
+        assert st.solved
+        assert S.shape == ref.shape
+        assert np.all(rel_cols(S, ref) < TOL), (gi, rel_cols(S, ref).max())
+        assert lat > 0
+    assert cnt["completed"] == len(reqs)
+    assert cnt["batches"] < len(reqs) and cnt["merged_requests"] > 0  # same-geometry requests merged
+    assert cnt["peak_inflight"] >= 2  # different geometries in flight together
+    assert cnt["queued"] == 0 and cnt["inflight"] == 0 and cnt["hbm_in_use"] == 0
+
+
+def test_server_plain_fp64_matches_gpu_solve(bie, stream):
+    ops, reqs = stream
+    gi, F = reqs[0]
+    ref, _ = bie.gpu_solve(ops[gi][1], F, rtol=1e-12, precision="fp64")
+    with bie.SolveServer(max_slots=1, max_batch_rhs=32) as srv:
+        t = srv.submit(ops[gi][1], F, rtol=1e-12, precision="fp64")
+        S, st, lat = srv.result(t)
+    assert np.all(rel_cols(S, ref) < 1e-12)
+
+
+def test_server_rejects_bad_requests(bie, stream):
+    ops, reqs = stream
+    from dielectricbie_jl_b200 import _abi
+    with bie.SolveServer(max_slots=1, max_batch_rhs=4) as srv:
+        F = np.zeros((ops[0][0].n, 5))
+        with pytest.raises(_abi.BieError):
+            srv.submit(ops[0][1], F)  # more columns than max_batch_rhs
+        with pytest.raises(_abi.BieError):
+            srv._shapes[12345] = (ops[0][0].n, 1, True)
+            srv.result(12345)  # unknown ticket
