@@ -42,7 +42,13 @@ WORKLOADS = {
                  up_tol=1e-9, max_order=8, probes=0, charges="pm1", inner=0.8),
     "cfg1": dict(box=(1.2, 0.8, 0.6), nq=4, l_ec=0.2, eps_in=4.0, eps_out=1.0, k=1, seed=1, rtol=1e-12,
                  up_tol=1e-9, max_order=8, probes=0, charges="one"),
+    # serving stream of uneven geometries (sides U[0.5, 2], eps_in log-U[2, 80], n_quad 4 or 6, node
+    # counts log-U[n_min, n_max], geometry repeats with p = 0.5, 1-32 point sources per request)
+    "cfg4": dict(requests=120, n_min=2000, n_max=30000, repeat=0.5, rate=200.0, seed=4, rtol=1e-8,
+                 up_tol=1e-9, max_order=8, k=0),
 }
+
+SERVE_CFG3 = dict(requests=192, rate=2000.0)  # single-source requests on the cfg3 box
 
 
 def load_package():
@@ -175,6 +181,10 @@ def run_reference_arm(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if "box" not in wl:
+        print(json.dumps({"impl": "reference", "unavailable": f"the CPU arm times single-geometry workloads; "
+                                                               f"{args.workload} is a multi-geometry stream"}))
+        return 0
     ref = CpuReference(wl)
     times, info = [], None
     for step in range(args.warmup + args.steps):
@@ -225,6 +235,150 @@ def profiled_traffic(name):
     return float(m.group(1)) if m else None
 
 
+def poisson_arrivals(rng, count, rate):
+    return np.cumsum(rng.exponential(1.0 / rate, size=count)) - 0.0
+
+
+def serve_stream(bie, requests, precision, rtol, slots=4, batch=64):
+    """Serves `requests` = [(op, F, arrival_s)] through the library's request server
+    (continuous batching), submitting each at its arrival time from a separate thread.
+    Latency = completion - arrival; throughput = RHS columns / (last completion - first arrival)."""
+    srv = bie.SolveServer(max_slots=slots, max_batch_rhs=batch)
+    nreq = len(requests)
+    tickets, sub_t = [None] * nreq, [0.0] * nreq
+    ready = [threading.Event() for _ in range(nreq)]
+    t0 = time.perf_counter() + 0.01
+
+    def submitter():
+        for i, (op, F, arr) in enumerate(requests):
+            dt = t0 + arr - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            sub_t[i] = time.perf_counter()
+            tickets[i] = srv.submit(op, F, rtol=rtol, precision=precision)
+            ready[i].set()
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    lat, done, cols, unsolved = [], [], 0, 0
+    for i in range(nreq):
+        ready[i].wait()
+        S, st, l_ms = srv.result(tickets[i])
+        t_done = sub_t[i] + l_ms * 1e-3
+        done.append(t_done)
+        lat.append((t_done - (t0 + requests[i][2])) * 1e3)
+        cols += requests[i][1].shape[1]
+        unsolved += int(not st.solved)
+    th.join()
+    cnt = srv.counters()
+    srv.close()
+    span = max(done) - (t0 + requests[0][2])
+    return {"solves_per_s": cols / span, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "requests": nreq, "solves": cols,
+            "unconverged_requests": unsolved, "batches": cnt["batches"], "merged_requests": cnt["merged_requests"],
+            "peak_inflight": cnt["peak_inflight"], "hbm_peak_bytes": cnt["hbm_peak"]}
+
+
+def plain_sequential(bie, requests, rtol):
+    """The plain FP64 GPU path one request at a time in arrival order (a request starts when
+    it has arrived and the previous one is done); same host API and copies as the server."""
+    t_free, lat, cols = 0.0, [], 0
+    for op, F, arr in requests:
+        start = max(arr, t_free)
+        t1 = time.perf_counter()
+        bie.gpu_solve(op, F, rtol=rtol, precision="fp64")
+        t_free = start + (time.perf_counter() - t1)
+        lat.append((t_free - arr) * 1e3)
+        cols += F.shape[1]
+    span = t_free - requests[0][2]
+    return {"solves_per_s": cols / span, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "requests": len(requests), "solves": cols}
+
+
+def cfg3_request_stream(bie, itf, op, wl, precision):
+    """Single-point-source requests on the cfg3 box, Poisson arrivals (seeded)."""
+    rng = np.random.default_rng(wl["seed"] + 100)
+    cnt, rate = SERVE_CFG3["requests"], SERVE_CFG3["rate"]
+    arr = poisson_arrivals(rng, cnt, rate)
+    half = np.array(wl["box"]) / 2 * 0.9
+    reqs = []
+    for i in range(cnt):
+        src = bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal()))
+        reqs.append((op, bie.rhs_dielectric_box3d(itf, [src], wl["eps_in"]), float(arr[i])))
+    served = serve_stream(bie, reqs, precision, wl["rtol"])
+    plain = plain_sequential(bie, reqs, wl["rtol"])
+    return {"workload": f"cfg3 request stream: {cnt} single-source requests, Poisson arrivals at {rate:g}/s "
+                        f"(seeded), rtol {wl['rtol']:g}",
+            "refined_served": served, "plain_fp64_sequential": plain,
+            "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"]}
+
+
+def box_for_nodes(bie, sides, nq, eps_in, target):
+    """l_ec by bisection on the mesher so that the box has about `target` nodes."""
+    lo, hi = 1e-3, 2.0 * max(sides)
+    best = None
+    for _ in range(30):
+        mid = math.sqrt(lo * hi)
+        itf = bie.single_dielectric_box3d(*sides, nq, mid, eps_in, 1.0)
+        if best is None or abs(math.log(itf.n / target)) < abs(math.log(best.n / target)):
+            best = itf
+        if itf.n > target:
+            lo = mid
+        else:
+            hi = mid
+        if hi / lo < 1.01:
+            break
+    return best
+
+
+def run_serving_workload(args, wl, bie, device):
+    """`--workload cfg4`: the uneven serving stream; served refined solver vs the plain FP64
+    path one request at a time. Geometries (mesh + near-field blocks) are built before the
+    timed stream and stay resident."""
+    rng = np.random.default_rng(wl["seed"])
+    geoms, reqs = [], []
+    arr = poisson_arrivals(rng, wl["requests"], wl["rate"])
+    for i in range(wl["requests"]):
+        if geoms and rng.random() < wl["repeat"]:
+            itf, op, eps_in = geoms[int(rng.integers(len(geoms)))]
+        else:
+            sides = tuple(float(v) for v in rng.uniform(0.5, 2.0, size=3))
+            eps_in = float(math.exp(rng.uniform(math.log(2.0), math.log(80.0))))
+            nq = int(rng.choice([4, 6]))
+            target = math.exp(rng.uniform(math.log(wl["n_min"]), math.log(wl["n_max"])))
+            itf = box_for_nodes(bie, sides, nq, eps_in, target)
+            op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, wl["up_tol"], wl["max_order"], device=device)
+            geoms.append((itf, op, eps_in))
+        k = int(rng.integers(1, 33))
+        half = 0.45 * (itf.corners.max(axis=(0, 1)) - itf.corners.min(axis=(0, 1)))
+        src = [bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal())) for _ in range(k)]
+        reqs.append((op, bie.rhs_dielectric_box3d(itf, src, eps_in), float(arr[i])))
+    # warm-up: one solve per geometry on each path (device buffers, kernel attributes)
+    for itf, op, eps_in in geoms:
+        F = np.ones((itf.n, 1))
+        bie.gpu_solve(op, F, rtol=1e-4, precision=args.precision)
+        bie.gpu_solve(op, F, rtol=1e-4, precision="fp64")
+    served = serve_stream(bie, reqs, args.precision, wl["rtol"])
+    plain = plain_sequential(bie, reqs, wl["rtol"])
+    nodes = [itf.n for itf, _, _ in geoms]
+    line = {"metric": METRIC, "value": served["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+            "steps": wl["requests"], "warmup": len(geoms), "ms_per_step": served["makespan_s"] * 1e3 / wl["requests"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": f"{args.precision} tensor-core direct sum + fp64",
+            "data": "synthetic (seeded boxes and point sources, Poisson arrivals)",
+            "config": {"workload": f"cfg4 serving stream (reduced): {wl['requests']} requests, node counts log-uniform "
+                                   f"in [{wl['n_min']}, {wl['n_max']}], {len(geoms)} distinct geometries "
+                                   f"(repeat p = {wl['repeat']}), 1-32 point sources each, Poisson arrivals "
+                                   f"{wl['rate']:g}/s, rtol {wl['rtol']:g}",
+                       "nodes_min": min(nodes), "nodes_max": max(nodes), "geometries": len(geoms),
+                       "geometry_setup": "mesh + near-field blocks built on the host before the timed stream"},
+            "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+            "refined_served": served, "plain_fp64_sequential": plain,
+            "speedup_vs_plain_fp64": served["solves_per_s"] / plain["solves_per_s"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def workload_config(name, wl, n):
     return {"workload": f"{name}: block {wl['k']}-RHS solve, box {'x'.join(str(v) for v in wl['box'])}, "
                         f"n_quad={wl['nq']}, l_ec={wl['l_ec']}, eps {wl['eps_in']}/{wl['eps_out']}, N={n}",
@@ -241,6 +395,7 @@ def main():
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the cfg3 request-stream measurement")
     ap.add_argument("--profile-matvec", action="store_true",
                     help="apply the refined and the FP64 operator once each to k columns and exit "
                          "(small case for ncu captures)")
@@ -266,6 +421,8 @@ def main():
     from dielectricbie_jl_b200 import _abi  # noqa: E402
     import ctypes as C
     L = _abi.lib()
+    if args.workload == "cfg4":
+        return run_serving_workload(args, wl, bie, device)
 
     # ---------------- setup (untimed): mesh, near-field blocks, device geometry -------
     itf = bie.single_dielectric_box3d(*wl["box"], wl["nq"], wl["l_ec"], wl["eps_in"], wl["eps_out"])
@@ -409,6 +566,11 @@ def main():
         (e2e_total,) = max_over_ranks(dist, [e2e_total], device)
     e2e_value = solves / (e2e_total * 1e-3)
 
+    # ---------------- serving: cfg3 request stream, continuous batching vs plain ------
+    serving = None
+    if args.workload == "cfg3" and world == 1 and not args.no_serving:
+        serving = cfg3_request_stream(bie, itf, op, wl, args.precision)
+
     # ---------------- roofline of the dominant kernel ------------------------------
     peaks = {}
     pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -479,6 +641,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": n * k * 8 + 5 * k * 8,
                     "d2h_bytes_per_step": 2 * n * k * 8},
+            "serving": serving,
             "gpu_launches": int(kt["all"].launches),
             "clocks": clocks,
         }
