@@ -38,6 +38,16 @@ struct bie_geom {
     std::vector<ProfRec> prof_pending;
     std::vector<cudaEvent_t> ev_pool;
     bie_kernel_time acc[BIE_KERNEL_KINDS] = {};
+    // CUDA graphs of GMRES iterations: one executable per Arnoldi step index j for the
+    // last two solver configurations (signature = sizes, options and buffer addresses)
+    struct GraphCache {
+        uint64_t sig = 0;
+        bool warm = false;  // one eager solve finished with these buffers: safe to capture
+        std::vector<cudaGraphExec_t> exec;
+    };
+    GraphCache gcache[2];
+    int gcache_next = 0;
+    bool graphs = true;  // off with the environment variable BIE_NO_GRAPHS
 };
 
 namespace bie {
@@ -445,10 +455,53 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
     g->jlast.ensure(sizeof(int) * k);
     g->yv.ensure(sizeof(double) * (size_t)m1 * k);
     g->resid.ensure(sizeof(double) * k);
+    {
+        // the column reductions' partials at their largest, so no iteration reallocates
+        size_t need = 0;
+        for (int nv = 1; nv <= m1; ++nv) {
+            const DotPlan p = dot_plan(n, k, nv);
+            need = std::max(need, (size_t)p.nblk * nv * k);
+        }
+        g->dpart.ensure(sizeof(double) * need);
+    }
     double* V = g->V.as<double>();
     double* W = g->W.as<double>();
     BIE_CK(cudaMemsetAsync(dx, 0, sizeof(double) * nk, s));
     upload(g->eps, eps.data(), k, s);
+
+    // Graph cache entry of this configuration. An iteration is captured once the same
+    // configuration has completed one eager solve (every buffer it touches is sized), and
+    // replayed afterwards; kernel timing (profiling) runs eagerly.
+    auto signature = [&]() {
+        uint64_t h = 1469598103934665603ull;
+        auto mix = [&](uint64_t v) {
+            h ^= v;
+            h *= 1099511628211ull;
+        };
+        mix((uint64_t)k); mix((uint64_t)prec); mix(flags); mix((uint64_t)m); mix((uintptr_t)pre);
+        const bie::Buf* bufs[] = {&g->V, &g->W, &g->part, &g->bpack, &g->dpart, &g->h, &g->h2, &g->hn, &g->R,
+                                  &g->cs, &g->sn, &g->gv, &g->active, &g->jlast, &g->eps, &g->resid, &g->errflag};
+        for (const auto* b : bufs) {
+            mix((uintptr_t)b->p);
+            mix((uint64_t)b->bytes);
+        }
+        return h;
+    };
+    const uint64_t sig0 = signature();
+    bie_geom::GraphCache* gc = nullptr;
+    for (auto& c : g->gcache)
+        if (c.sig == sig0 && !c.exec.empty()) gc = &c;
+    if (!gc) {
+        gc = &g->gcache[g->gcache_next];
+        g->gcache_next ^= 1;
+        for (auto ex : gc->exec)
+            if (ex) cudaGraphExecDestroy(ex);
+        gc->sig = sig0;
+        gc->warm = false;
+        gc->exec.assign(m, nullptr);
+    }
+    bool use_graph = g->graphs && !g->prof_on && gc->warm && s == g->stream;
+
     GmresResult res;
     res.col_iters.assign(k, 0);
     std::vector<double> hb(k), g0((size_t)k);
@@ -491,29 +544,57 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
         int j = 0;
         bool any = true;
         for (; j < m && it < itmax; ++j) {
-            double* Vj = V + (size_t)j * nk;
-            apply_op(g, Vj, W, k, prec, flags, pre, s);
+            auto iteration = [&]() {
+                double* Vj = V + (size_t)j * nk;
+                apply_op(g, Vj, W, k, prec, flags, pre, s);
+                // classical Gram-Schmidt, twice; the second pass is fused with the norm of the
+                // new direction and its coefficients are added to the first pass's in the Givens step
+                dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
+                {
+                    Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                    k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+                }
+                dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
+                gs_update_norm(g, W, V, nk, j + 1, g->h2.as<double>(), k, g->hn.as<double>(), s);
+                {
+                    Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                    k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
+                }
+                {
+                    Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                    k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->h2.as<double>(),
+                                                        g->hn.as<double>(), g->cs.as<double>(), g->sn.as<double>(),
+                                                        g->gv.as<double>(), g->active.as<int>(), g->jlast.as<int>(),
+                                                        g->eps.as<double>(), g->resid.as<double>(), j, m1, k);
+                }
+                BIE_CK(cudaGetLastError());
+            };
             ++res.matvecs;
-            // classical Gram-Schmidt, twice; the second pass is fused with the norm of the
-            // new direction and its coefficients are added to the first pass's in the Givens step
-            dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
-            {
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+            if (use_graph && !gc->exec[j]) {
+                // capture iteration j; on any failure fall back to eager iterations
+                BIE_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                bool ok = true;
+                try {
+                    iteration();
+                } catch (...) {
+                    ok = false;
+                }
+                cudaGraph_t graph = nullptr;
+                const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+                cudaGraphExec_t ex = nullptr;
+                if (ok && ec == cudaSuccess && graph && cudaGraphInstantiate(&ex, graph, 0) == cudaSuccess)
+                    gc->exec[j] = ex;
+                if (graph) cudaGraphDestroy(graph);
+                if (!gc->exec[j]) {
+                    cudaGetLastError();
+                    use_graph = false;
+                    g->graphs = false;
+                }
             }
-            dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
-            gs_update_norm(g, W, V, nk, j + 1, g->h2.as<double>(), k, g->hn.as<double>(), s);
-            {
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
-            }
-            {
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->h2.as<double>(),
-                                                    g->hn.as<double>(), g->cs.as<double>(), g->sn.as<double>(),
-                                                    g->gv.as<double>(), g->active.as<int>(), g->jlast.as<int>(),
-                                                    g->eps.as<double>(), g->resid.as<double>(), j, m1, k);
-            }
+            if (use_graph)
+                BIE_CK(cudaGraphLaunch(gc->exec[j], s));
+            else
+                iteration();
             BIE_CK(cudaGetLastError());
             ++it;
             if ((j + 1) % std::max(1, check_every) == 0 || j + 1 == m || it >= itmax) {
@@ -548,6 +629,7 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
         if (it >= itmax) break;
         first = false;  // restart from the true residual of the current iterate
     }
+    if (signature() == gc->sig) gc->warm = true;
     res.iters = it;
     return res;
 }
@@ -586,6 +668,7 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
     DeviceGuard dg(device);
     std::unique_ptr<bie_geom> g(new bie_geom());
     g->device = device;
+    g->graphs = std::getenv("BIE_NO_GRAPHS") == nullptr;
     BIE_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     BIE_CK(cudaEventCreate(&g->ev0));
     BIE_CK(cudaEventCreate(&g->ev1));
@@ -669,6 +752,9 @@ void geom_destroy(bie_geom* g) {
             cudaEventDestroy(r.b);
         }
         for (auto e : g->ev_pool) cudaEventDestroy(e);
+        for (auto& c : g->gcache)
+            for (auto ex : c.exec)
+                if (ex) cudaGraphExecDestroy(ex);
         if (g->ev0) cudaEventDestroy(g->ev0);
         if (g->ev1) cudaEventDestroy(g->ev1);
         if (g->stream) cudaStreamDestroy(g->stream);
