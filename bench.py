@@ -684,7 +684,8 @@ def main():
                     "peak_source": f"bf16_tflops_sustained {peak_src}",
                     "traffic": profiled_traffic(f"k_dt_tc_{args.workload}.md"),
                     "traffic_source": f"profiles/k_dt_tc_{args.workload}.md (ncu dram bytes read + written per launch)",
-                    "per_launch_ms": per_launch_ms}
+                    "per_launch_ms": per_launch_ms,
+                    "autotuned_launch": bie.tuned_launch(op, "tensor_core", k)}
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         fp32_issue_peak = 148 * 128 * sm_mhz * 1e6  # FP32 lane-instructions/s at the sampled clock
         pairs_per_s = tc.pairs / (tc.launches / 2) / (per_launch_ms * 1e-3)

@@ -355,6 +355,20 @@ int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int3
     });
 }
 
+int bie_tuning_read(bie_geom* g, int32_t family, int32_t columns, int32_t pieces, int32_t* nsplit,
+                    int32_t* ctas_per_sm, double* ms) {
+    return guarded([&] {
+        REQUIRE(g && nsplit && ctas_per_sm && ms, "tuning_read: bad argument");
+        int ns = 0, ct = 0;
+        double t = 0.0;
+        if (!bie::tuning_read(g, family, columns, pieces, &ns, &ct, &t))
+            throw Error(BIE_EINVAL, "tuning_read: no tuned configuration for this key");
+        *nsplit = ns;
+        *ctas_per_sm = ct;
+        *ms = t;
+    });
+}
+
 void bie_server_opts_default(bie_server_opts* o) {
     if (!o) return;
     o->max_slots = 4;

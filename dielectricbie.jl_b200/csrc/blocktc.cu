@@ -683,10 +683,12 @@ struct Shape {
     size_t smem;
 };
 
-Shape shape(int npad, int np) {
+// force_ctas = 1 or 2 selects that shape when it fits (0 = the default choice).
+Shape shape(int npad, int np, int force_ctas = 0) {
     const size_t half_sm = 113 * 1024;  // 228 KB per SM, 1 KB reserved per CTA
     Shape sh;
-    if (tmem_cols(npad) <= 256 && smem_bytes(npad, np, 2, 2) <= half_sm) {
+    const bool two = tmem_cols(npad) <= 256 && smem_bytes(npad, np, 2, 2) <= half_sm;
+    if (two && force_ctas != 1) {
         sh.ctas = 2;
         sh.nq = 2;
         sh.sa = 2;
@@ -710,7 +712,7 @@ void launch_k(const Params& P, dim3 grid, size_t sm, cudaStream_t s) {
 
 template <int NP>
 void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit, int64_t cps,
-               float* part, int ldp, uint8_t* bpack, int* err, cudaStream_t s) {
+               float* part, int ldp, uint8_t* bpack, int* err, int force_ctas, cudaStream_t s) {
     const int npad = ((kc + 15) / 16) * 16;
     const int64_t nchunks = (g.n + KC - 1) / KC;
     const int64_t pk = nchunks * npad * 8;
@@ -723,7 +725,7 @@ void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const
     P.keff = kc;
     P.nchunks = nchunks;
     P.cps = cps;
-    const Shape sh = shape(npad, NP);
+    const Shape sh = shape(npad, NP, force_ctas);
     P.sa = sh.sa;
     P.sb = sh.sb;
     P.part = part;
@@ -745,11 +747,12 @@ int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
 // with the kernel and right-hand sides split into `pieces` (2: three products,
 // 3: six products) bf16 pieces.
 void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
-                     int64_t cps, float* part, int ldp, uint8_t* bpack, int* err, int pieces, cudaStream_t s) {
+                     int64_t cps, float* part, int ldp, uint8_t* bpack, int* err, int pieces, int force_ctas,
+                     cudaStream_t s) {
     if (pieces == 3)
-        tc::launch_tc<3>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, s);
+        tc::launch_tc<3>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, force_ctas, s);
     else
-        tc::launch_tc<2>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, s);
+        tc::launch_tc<2>(g, X, ldx, c0, kc, pre, nsplit, cps, part, ldp, bpack, err, force_ctas, s);
 }
 
 size_t block_tc_pack_bytes(int64_t n, int kc, int pieces) {
@@ -757,6 +760,8 @@ size_t block_tc_pack_bytes(int64_t n, int kc, int pieces) {
     return (size_t)nchunks * pieces * tc_npad(kc) * 128;
 }
 
-int block_tc_ctas_per_sm(int kc, int pieces) { return tc::shape(tc_npad(kc), pieces).ctas; }
+int block_tc_ctas_per_sm(int kc, int pieces, int force_ctas) {
+    return tc::shape(tc_npad(kc), pieces, force_ctas).ctas;
+}
 
 }  // namespace bie

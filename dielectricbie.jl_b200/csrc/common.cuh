@@ -31,9 +31,10 @@ struct GeomDev {
 // K3 (blocktc.cu): tensor-core block direct sum for columns [c0, c0 + kc), kc <= 128,
 // kernel and right-hand sides split into `pieces` bf16 pieces (2 or 3).
 void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,
-                     int64_t cps, float* part, int ldp, uint8_t* bpack, int* err, int pieces, cudaStream_t s);
+                     int64_t cps, float* part, int ldp, uint8_t* bpack, int* err, int pieces, int force_ctas,
+                     cudaStream_t s);
 size_t block_tc_pack_bytes(int64_t n, int kc, int pieces);
-int block_tc_ctas_per_sm(int kc, int pieces);
+int block_tc_ctas_per_sm(int kc, int pieces, int force_ctas = 0);
 int tc_npad(int kc);
 // K1 with the FP64 tensor-core contraction (dt64mma.cu), columns [c0, c0 + kc), kc <= 64.
 void launch_dt_f64_mma(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit,

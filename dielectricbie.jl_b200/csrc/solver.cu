@@ -2,6 +2,10 @@
 // iterative-refinement solvers of libbie_b200.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <memory>
+#include <tuple>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -48,6 +52,15 @@ struct bie_geom {
     GraphCache gcache[2];
     int gcache_next = 0;
     bool graphs = true;  // off with the environment variable BIE_NO_GRAPHS
+    // autotuned launch configurations of the direct sums, keyed by (family, columns, pieces)
+    struct Tuned {
+        int nsplit;
+        int64_t chunk;
+        int ctas;
+        double ms;
+    };
+    std::map<std::tuple<int, int, int>, Tuned> tuned;
+    bool autotune = true;  // off with the environment variable BIE_NO_AUTOTUNE
 };
 
 namespace bie {
@@ -221,19 +234,89 @@ int pick_C(int rem) {
 }
 
 // Runs the direct sum for all k columns into g->part; returns the split used.
+// K1 (FP64 tensor-core) split with ns source splits (chunks rounded up to kTS sources).
+Split dt64_split_n(const bie_geom* g, int64_t ns) {
+    ns = std::max<int64_t>(1, std::min<int64_t>(ns, (g->n + kTS - 1) / kTS));
+    int64_t chunk = (g->n + ns - 1) / ns;
+    chunk = (chunk + kTS - 1) / kTS * kTS;
+    return Split{(int)((g->n + chunk - 1) / chunk), chunk};
+}
+
+// Autotuning is allowed on an eager, unprofiled stream.
+bool can_tune(const bie_geom* g, cudaStream_t s) {
+    if (!g->autotune || g->prof_on) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+// Device time (ms) of one call of `run` on stream s.
+template <class F>
+double time_on(bie_geom* g, cudaStream_t s, F&& run) {
+    if (!g->ev0) BIE_CK(cudaEventCreate(&g->ev0));
+    if (!g->ev1) BIE_CK(cudaEventCreate(&g->ev1));
+    BIE_CK(cudaEventRecord(g->ev0, s));
+    run();
+    BIE_CK(cudaEventRecord(g->ev1, s));
+    BIE_CK(cudaEventSynchronize(g->ev1));
+    float ms = 0.f;
+    BIE_CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    return ms;
+}
+
+// Autotuner: times the candidate launch configurations on the real operand once
+// per (family, columns, pieces) and keeps the fastest; the wave model's choice is
+// kept unless another candidate is more than 2 % faster.
+template <class Launch>
+bie_geom::Tuned tune(bie_geom* g, cudaStream_t s, const std::vector<bie_geom::Tuned>& cands, Launch&& launch) {
+    launch(cands.front());  // warm-up (first-use costs)
+    std::vector<double> t(cands.size());
+    for (size_t i = 0; i < cands.size(); ++i) t[i] = time_on(g, s, [&] { launch(cands[i]); });
+    size_t best = 0;
+    for (size_t i = 1; i < cands.size(); ++i)
+        if (t[i] < t[best]) best = i;
+    if (t[best] > 0.98 * t[0]) best = 0;
+    bie_geom::Tuned r = cands[best];
+    r.ms = t[best];
+    return r;
+}
+
 Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const double* pre, const double* T,
                  int64_t M, cudaStream_t s) {
     GeomDev gd = gdev(g);
     if (kind == Kern::DT64 && k >= 8) {
-        // FP64 tensor-core contraction, 64 columns per launch, 2 CTAs of 128 targets per SM
-        Split sp = choose_split(g->n, g->n, g->sms, 2);
-        g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
+        // FP64 tensor-core contraction, 64 columns per launch, 2 CTAs of 128 targets per SM;
+        // the source split count is autotuned around the occupancy model's
         const double npairs = (double)g->n * (g->n - 1);
-        for (int c0 = 0; c0 < k; c0 += 64) {
-            const int kc = std::min(64, k - c0);
-            Prof pf(g, BIE_KERNEL_DIRECT_FP64, s, 1, npairs, npairs * kc);
-            launch_dt_f64_mma(gd, X, ldx, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, s);
+        auto run = [&](const Split& sp, bool prof) {
+            g->part.ensure(sizeof(double) * (size_t)sp.nsplit * g->n * k);
+            for (int c0 = 0; c0 < k; c0 += 64) {
+                const int kc = std::min(64, k - c0);
+                std::unique_ptr<Prof> pf;
+                if (prof) pf.reset(new Prof(g, BIE_KERNEL_DIRECT_FP64, s, 1, npairs, npairs * kc));
+                launch_dt_f64_mma(gd, X, ldx, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, s);
+            }
+        };
+        const Split base = choose_split(g->n, g->n, g->sms, 2);
+        const auto key = std::make_tuple(1, std::min(k, 64), 0);
+        auto it = g->tuned.find(key);
+        if (it == g->tuned.end() && can_tune(g, s)) {
+            std::vector<bie_geom::Tuned> cands{{base.nsplit, base.chunk, 2, 0.0}};
+            for (int64_t ns : {(int64_t)base.nsplit / 2, 2 * (int64_t)base.nsplit}) {
+                const Split sp = dt64_split_n(g, ns);
+                bool dup = false;
+                for (auto& c : cands) dup = dup || c.nsplit == sp.nsplit;
+                if (!dup) cands.push_back({sp.nsplit, sp.chunk, 2, 0.0});
+            }
+            it = g->tuned.emplace(key, tune(g, s, cands, [&](const bie_geom::Tuned& c) {
+                                       run(Split{c.nsplit, c.chunk}, false);
+                                   })).first;
         }
+        const Split sp = it != g->tuned.end() ? Split{it->second.nsplit, it->second.chunk} : base;
+        run(sp, true);
         return sp;
     }
     int64_t rows = kind == Kern::POT64 ? M : g->n;
@@ -264,11 +347,12 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
 // K3 launch plan: the number of source splits ns (<= 16, and at most 1024 chunks
 // per split) that minimises the time of the wave-quantised grid, which is
 // proportional to ceil(tiles ns / slots) / ns; ties go to fewer splits (each
-// split adds an FP32 partial for the combine to read).
-Split tc_split(const bie_geom* g, int kc, int pieces) {
+// split adds an FP32 partial for the combine to read). force_ctas selects the CTA
+// shape (0 = default).
+Split tc_split(const bie_geom* g, int kc, int pieces, int force_ctas = 0) {
     const int64_t tiles = (g->n + kTcTileM - 1) / kTcTileM;
     const int64_t chunks = (g->n + kTcChunk - 1) / kTcChunk;
-    const int64_t slots = (int64_t)g->sms * block_tc_ctas_per_sm(kc, pieces);
+    const int64_t slots = (int64_t)g->sms * block_tc_ctas_per_sm(kc, pieces, force_ctas);
     const int64_t ns_min = std::min<int64_t>(chunks, std::max<int64_t>(1, (chunks + 1023) / 1024));
     const int64_t ns_max = std::min<int64_t>(chunks, std::max<int64_t>(ns_min, 16));
     int64_t ns = ns_min;
@@ -288,18 +372,57 @@ Split tc_split(const bie_geom* g, int kc, int pieces) {
     return Split{(int)ns, cps};
 }
 
+// K3 split with ns source splits (chunks per split rounded up).
+Split tc_split_n(const bie_geom* g, int64_t ns) {
+    const int64_t chunks = (g->n + kTcChunk - 1) / kTcChunk;
+    ns = std::max<int64_t>(std::max<int64_t>(1, (chunks + 1023) / 1024), std::min(ns, chunks));
+    const int64_t cps = (chunks + ns - 1) / ns;
+    return Split{(int)((chunks + cps - 1) / cps), cps};
+}
+
 Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, int pieces, cudaStream_t s) {
     GeomDev gd = gdev(g);
-    Split sp = tc_split(g, std::min(k, 128), pieces);
-    g->part.ensure(sizeof(float) * (size_t)sp.nsplit * g->n * k);
-    g->bpack.ensure(block_tc_pack_bytes(g->n, std::min(k, 128), pieces));
-    for (int c0 = 0; c0 < k; c0 += 128) {
-        int kc = std::min(128, k - c0);
-        const double npairs = (double)g->n * (g->n - 1);
-        Prof pf(g, BIE_KERNEL_DIRECT_TC, s, 2, npairs, npairs * tc_npad(kc));
-        launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<float>(), k, g->bpack.as<uint8_t>(),
-                        g->errflag.as<int>(), pieces, s);
+    const int kc0 = std::min(k, 128);
+    const double npairs = (double)g->n * (g->n - 1);
+    auto run = [&](const Split& sp, int ctas, bool prof) {
+        g->part.ensure(sizeof(float) * (size_t)sp.nsplit * g->n * k);
+        g->bpack.ensure(block_tc_pack_bytes(g->n, kc0, pieces));
+        for (int c0 = 0; c0 < k; c0 += 128) {
+            int kc = std::min(128, k - c0);
+            std::unique_ptr<Prof> pf;
+            if (prof) pf.reset(new Prof(g, BIE_KERNEL_DIRECT_TC, s, 2, npairs, npairs * tc_npad(kc)));
+            launch_block_tc(gd, X, k, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<float>(), k,
+                            g->bpack.as<uint8_t>(), g->errflag.as<int>(), pieces, ctas, s);
+        }
+    };
+    const auto key = std::make_tuple(0, kc0, pieces);
+    auto it = g->tuned.find(key);
+    if (it == g->tuned.end() && can_tune(g, s)) {
+        std::vector<bie_geom::Tuned> cands;
+        const int shape0 = block_tc_ctas_per_sm(kc0, pieces, 0);
+        for (int ctas : {shape0, shape0 == 2 ? 1 : 0}) {
+            if (ctas == 0) continue;
+            const Split base = tc_split(g, kc0, pieces, ctas);
+            for (int64_t ns : {(int64_t)base.nsplit, (int64_t)base.nsplit / 2, 2 * (int64_t)base.nsplit}) {
+                const Split sp = ns == base.nsplit ? base : tc_split_n(g, ns);
+                bool dup = false;
+                for (auto& c : cands) dup = dup || (c.nsplit == sp.nsplit && c.ctas == ctas);
+                if (!dup) cands.push_back({sp.nsplit, sp.chunk, ctas, 0.0});
+            }
+        }
+        it = g->tuned.emplace(key, tune(g, s, cands, [&](const bie_geom::Tuned& c) {
+                                   run(Split{c.nsplit, c.chunk}, c.ctas, false);
+                               })).first;
     }
+    Split sp;
+    int ctas = 0;
+    if (it != g->tuned.end()) {
+        sp = Split{it->second.nsplit, it->second.chunk};
+        ctas = it->second.ctas;
+    } else {
+        sp = tc_split(g, kc0, pieces);
+    }
+    run(sp, ctas, true);
     return sp;
 }
 
@@ -669,6 +792,7 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
     std::unique_ptr<bie_geom> g(new bie_geom());
     g->device = device;
     g->graphs = std::getenv("BIE_NO_GRAPHS") == nullptr;
+    g->autotune = std::getenv("BIE_NO_AUTOTUNE") == nullptr;
     BIE_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     BIE_CK(cudaEventCreate(&g->ev0));
     BIE_CK(cudaEventCreate(&g->ev1));
@@ -736,6 +860,15 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
                                                                      sizeof(double) * (size_t)nblocks * nb * nb)
                                                                   : 0);
     return g.release();
+}
+
+bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, int* ctas, double* ms) {
+    auto it = g->tuned.find(std::make_tuple(family, columns, pieces));
+    if (it == g->tuned.end()) return false;
+    *nsplit = it->second.nsplit;
+    *ctas = it->second.ctas;
+    *ms = it->second.ms;
+    return true;
 }
 
 void geom_destroy(bie_geom* g) {

@@ -42,6 +42,7 @@ void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes);
 void* geom_stream(bie_geom* g);
 void profile_enable(bie_geom* g, int on);
 void profile_read(bie_geom* g, int kind, bie_kernel_time* out);
+bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, int* ctas, double* ms);
 
 void matvec_host(bie_geom* g, const double* X, double* Y, int k, int precision, uint32_t flags);
 void matvec_device(bie_geom* g, const double* dX, double* dY, int k, int precision, uint32_t flags, cudaStream_t s);

@@ -257,6 +257,16 @@ int bie_profile_enable(bie_geom* g, int enable);
 /* Reads the accumulated figures of one kernel kind (synchronises the stream). */
 int bie_profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 
+/* Autotuned launch configuration of a direct-sum family on this geometry: family 0 =
+ * tensor-core block sum (columns = min(k, 128), pieces 2 or 3), 1 = FP64 tensor-core
+ * sum (columns = min(k, 64), pieces 0). The library times a few candidate launch
+ * shapes (CTA shape, source split count) on the first application of each family and
+ * column width and keeps the fastest (environment variable BIE_NO_AUTOTUNE turns this
+ * off). Returns BIE_EINVAL when nothing was tuned for the key. No counterpart in the
+ * reference (its FMM has no launch shapes). */
+int bie_tuning_read(bie_geom* g, int32_t family, int32_t columns, int32_t pieces, int32_t* nsplit,
+                    int32_t* ctas_per_sm, double* ms);
+
 /* ---- request server: the serving loop around the block solve -------------------
  * Requests of solve_dielectric_box3d_block (src/solver/multi_rhs.jl:270-286) --
  * a geometry handle, an N x k block of right-hand sides and solver options -- are

@@ -213,3 +213,19 @@ def test_combine_column_tiles(bie, cfg1, rng, k):
     Y = op @ X
     ref = A @ X + Cm @ X
     assert rel(Y, ref) < 1e-13
+
+
+def test_autotuned_launch_recorded_and_accurate(bie, cfg1, rng):
+    """The first tensor-core and FP64 applications tune their launch shape; results stay
+    within the operators' bars (the split count only changes the partial-sum rounding)."""
+    itf, m, Cm, A = cfg1
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, 1e-9, 8)
+    X = rng.standard_normal((itf.n, 24))
+    Y64 = op.mul(X)
+    Y3 = op.mul(X, precision="bf16x3")
+    t_tc = bie.tuned_launch(op, "tensor_core", 24)
+    t_64 = bie.tuned_launch(op, "fp64", 24)
+    assert t_tc is not None and t_tc["nsplit"] >= 1 and t_tc["ctas_per_sm"] in (1, 2) and t_tc["ms"] > 0
+    assert t_64 is not None and t_64["nsplit"] >= 1
+    assert rel(Y64, A @ X + Cm @ X) < 1e-13
+    assert rel(Y3, Y64) < 5e-5
