@@ -33,6 +33,7 @@
 // returns after releasing its tensor memory.
 #include <cuda_bf16.h>
 #include <algorithm>
+#include <cstdlib>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -60,7 +61,7 @@ __host__ __device__ inline uint32_t tmem_cols(int npad) {
     return c;
 }
 constexpr int FP = 4;          // chunks accumulated in FP32 tensor memory before a compensated fold
-constexpr uint32_t kWaitLimit = 1u << 26;  // wait attempts before a CTA gives up (seconds)
+constexpr uint32_t kWaitLimit = 1u << 26;  // default wait attempts before a CTA gives up (seconds)
 constexpr int kErrTimeout = 1;
 
 struct Params {
@@ -71,6 +72,8 @@ struct Params {
     int64_t nchunks;
     int64_t cps;           // chunks per split
     int sa, sb;            // A and B ring stages (2 .. SAMAX, 2 .. SBMAX)
+    uint32_t wait_limit;   // mbarrier wait attempts before the CTA gives up
+    int stall_test;        // nonzero: withhold the first Q tile (exercises the timeout path)
     float* part;           // [nsplit][n][ldp] FP32 split partials
     int ldp, c0;
     int* err;
@@ -104,8 +107,8 @@ __device__ __forceinline__ bool flag_set(volatile int* f) {
     return v != 0;
 }
 // Bounded wait; returns false (and flags the CTA) when the limit expires.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try(b, parity)) return true;
         if (flag_set(abort_flag)) return false;
     }
@@ -114,8 +117,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
 }
 
 // Wait bounded by an iteration limit only (used to drain in-flight work on the abort path).
-__device__ __forceinline__ bool mbar_wait_raw(uint64_t* b, uint32_t parity) {
-    for (uint32_t it = 0; it < kWaitLimit; ++it)
+__device__ __forceinline__ bool mbar_wait_raw(uint64_t* b, uint32_t parity, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try(b, parity)) return true;
     return false;
 }
@@ -448,7 +451,7 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
         // decides as a whole.
         auto fold = [&](int p) -> bool {
             const int b = p & 1;
-            bool ok = mbar_wait(&acc_full[b], (uint32_t)(p >> 1) & 1u, abort_flag);
+            bool ok = mbar_wait(&acc_full[b], (uint32_t)(p >> 1) & 1u, abort_flag, P.wait_limit);
             if (!__all_sync(full, ok)) return false;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             for (int c = qt * 16; c < npad; c += 16 * NQ) {
@@ -477,8 +480,8 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
             const int s = lc % SA, sc = lc % SC;
             const int64_t j0 = (ch0 + lc) * KC;
             // coordinates staged; A stage s released by the MMAs of chunk lc - S
-            if (!mbar_wait(&crd_full[sc], (uint32_t)(lc / SC) & 1u, abort_flag)) { ok = false; break; }
-            if (lc >= SA && !mbar_wait(&empty_a[s], (uint32_t)(lc / SA - 1) & 1u, abort_flag)) { ok = false; break; }
+            if (!mbar_wait(&crd_full[sc], (uint32_t)(lc / SC) & 1u, abort_flag, P.wait_limit)) { ok = false; break; }
+            if (lc >= SA && !mbar_wait(&empty_a[s], (uint32_t)(lc / SA - 1) & 1u, abort_flag, P.wait_limit)) { ok = false; break; }
             uint8_t* As = A + s * NP * a_bytes;
             const float* cs = crd + sc * 3 * KC;
             const bool self = (i >= j0) && (i < j0 + KC);  // this chunk holds the target's own node
@@ -528,10 +531,10 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
                 const int s = lc % SA, sb = lc % SB;
                 const int p = lc / FP, b = p & 1;
                 const bool pfirst = (lc % FP) == 0;
-                if (!mbar_wait(&full_a[s], (uint32_t)(lc / SA) & 1u, abort_flag)) break;
-                if (!mbar_wait(&full_b[sb], (uint32_t)(lc / SB) & 1u, abort_flag)) break;
+                if (!mbar_wait(&full_a[s], (uint32_t)(lc / SA) & 1u, abort_flag, P.wait_limit)) break;
+                if (!mbar_wait(&full_b[sb], (uint32_t)(lc / SB) & 1u, abort_flag, P.wait_limit)) break;
                 // accumulator b is reused from period p - 2 once the generators folded it
-                if (pfirst && p >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)((p - 2) >> 1) & 1u, abort_flag)) break;
+                if (pfirst && p >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)((p - 2) >> 1) & 1u, abort_flag, P.wait_limit)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 // descriptors of the stage; the start-address field (bits 0-13, address >> 4)
                 // is advanced in place: every address stays below 256 KB
@@ -557,7 +560,7 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
             }
             mma_commit(acc_done);
             // on abort, drain this thread's MMAs before the CTA releases tensor memory
-            if (*abort_flag) mbar_wait_raw(acc_done, 0);
+            if (*abort_flag) mbar_wait_raw(acc_done, 0, P.wait_limit);
         }
         __syncwarp();
     } else {
@@ -569,10 +572,12 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
         int issued = 0;
         auto stage_b = [&](int c) -> bool {
             const int sb = c % SB;
-            if (c >= SB && !mbar_wait(&empty_b[sb], (uint32_t)(c / SB - 1) & 1u, abort_flag)) return false;
+            if (c >= SB && !mbar_wait(&empty_b[sb], (uint32_t)(c / SB - 1) & 1u, abort_flag, P.wait_limit)) return false;
             if (lane == 0) {
                 mbar_arrive_tx(&full_b[sb], bytes);
-                bulk_g2s(B + sb * NP * b_bytes, P.bpack + (size_t)(ch0 + c) * bytes, bytes, &full_b[sb]);
+                // test of the timeout path: the first Q tile is announced but never copied
+                if (!(P.stall_test && c == 0))
+                    bulk_g2s(B + sb * NP * b_bytes, P.bpack + (size_t)(ch0 + c) * bytes, bytes, &full_b[sb]);
                 issued = c + 1;
             }
             return true;
@@ -591,7 +596,7 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
                 }
             }
             const int sc = c % SC;
-            if (c >= SC && !mbar_wait(&crd_empty[sc], (uint32_t)(c / SC - 1) & 1u, abort_flag)) return false;
+            if (c >= SC && !mbar_wait(&crd_empty[sc], (uint32_t)(c / SC - 1) & 1u, abort_flag, P.wait_limit)) return false;
             float* cs = crd + sc * 3 * KC;
 #pragma unroll
             for (int h = 0; h < KC / 32; ++h) {
@@ -610,7 +615,8 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
         }
         // on abort, wait for the copies still in flight (at most one per slot)
         if (lane == 0 && *abort_flag)
-            for (int c = issued > SB ? issued - SB : 0; c < issued; ++c) mbar_wait_raw(&full_b[c % SB], (c / SB) & 1);
+            for (int c = issued > SB ? issued - SB : 0; c < issued; ++c)
+                if (!(P.stall_test && c == 0)) mbar_wait_raw(&full_b[c % SB], (c / SB) & 1, P.wait_limit);
         __syncwarp();
     }
 
@@ -726,6 +732,10 @@ void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const
     P.nchunks = nchunks;
     P.cps = cps;
     const Shape sh = shape(npad, NP, force_ctas);
+    // BIE_TEST_TC_STALL (tests only): every CTA's first Q tile never arrives, so the
+    // bounded waits expire quickly and the launch reports a timeout
+    P.stall_test = std::getenv("BIE_TEST_TC_STALL") != nullptr;
+    P.wait_limit = P.stall_test ? (1u << 14) : kWaitLimit;
     P.sa = sh.sa;
     P.sb = sh.sb;
     P.part = part;
