@@ -546,13 +546,15 @@ def main():
         o.flags = 0 if verify else _abi.BIE_NO_VERIFY
         return o
 
-    def solve_step(i, precision, rtol, verify=False, st=None):
+    def solve_step(i, precision, rtol, verify=False, st=None, allow_noconv=False):
         _abi.check(L.bie_rhs_point_device(g, C.c_void_p(src_d[i].data_ptr()), C.c_void_p(q_d[i].data_ptr()),
                                           C.c_void_p(eps_d.data_ptr()), k, C.c_void_p(F.data_ptr()), None))
         o = opts(precision, rtol, verify)
+        if allow_noconv:
+            o.itmax = 1500
         rc = L.bie_solve_device(g, C.c_void_p(F.data_ptr()), C.c_void_p(S.data_ptr()), k, C.byref(o),
                                 C.byref(st) if st is not None else None, None)
-        if rc != _abi.BIE_OK:
+        if rc != _abi.BIE_OK and not (allow_noconv and rc == _abi.BIE_ENOCONV):
             _abi.check(rc)
 
     def timed_loop(precision, rtol, tag, profile=False):
@@ -578,10 +580,13 @@ def main():
 
     # ---------------- accuracy (untimed): refined vs plain FP64 on the same batch -----
     st = _abi.Stats()
-    solve_step(nsteps, "fp64", 1e-13, verify=True, st=st)
+    # reference: plain FP64 at rtol 1e-13 (at high contrast it may stop at its FP64 floor
+    # first; the residual it reached is reported)
+    solve_step(nsteps, "fp64", 1e-13, verify=True, st=st, allow_noconv=True)
     torch.cuda.synchronize(device)
     S_ref = S.cpu().numpy().copy()
     plain_ref_iters = st.iterations
+    ref_resid = st.max_rel_resid
     solve_step(nsteps, args.precision, wl["rtol"], verify=True, st=st)
     torch.cuda.synchronize(device)
     S_ref_refined = S.cpu().numpy().copy()
@@ -589,7 +594,8 @@ def main():
     accuracy = {"sigma_rel_err_max": sig_err, "refined_true_rel_resid": st.max_rel_resid,
                 "refined_iterations": st.iterations, "refined_outer": st.outer,
                 "refined_fp64_matvecs": st.fp64_matvecs, "refined_lowp_matvecs": st.lowp_matvecs,
-                "reference_sigma": "plain FP64 GPU solve at rtol 1e-13"}
+                "reference_sigma": "plain FP64 GPU solve at rtol 1e-13",
+                "reference_true_rel_resid": ref_resid}
     pos, qs = batches[nsteps]
     if wl["probes"]:
         T = make_probes(bie, itf, wl["probes"], wl["seed"])

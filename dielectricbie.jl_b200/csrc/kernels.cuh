@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace bie {
@@ -294,16 +296,22 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 constexpr int kCombTile = 32;  // columns per CTA
-constexpr int kCombLDX = 36;   // slab row stride (doubles): 32 + 4, conflict-free fragment loads
 
-// Shared memory of the block-row combine for nb-row panels.
-inline size_t combine_smem_bytes(int nb) {
+// Slab row stride for a kt-column tile: kt rounded up to 8, plus 4 (stride = 4 or 12
+// mod 16 doubles, so a half-warp's fragment loads hit distinct banks).
+__host__ __device__ inline int comb_ldx(int kt) { return ((kt + 7) / 8) * 8 + 4; }
+
+// Shared memory of the block-row combine for nb-row panels, kt-column tiles and
+// `stages` pipeline stages (reused for the warps' final reduction).
+inline size_t combine_smem_bytes(int nb, int kt, int stages) {
     const int mt = (nb + 7) / 8, kp = ((nb + 3) / 4) * 4;
     const int ldc = mt * 8 + 4;
-    return sizeof(double) * (2 * (size_t)kp * ldc + 2 * (size_t)kp * kCombLDX + 2 * (size_t)kp);
+    const size_t pipe = (size_t)stages * kp * (ldc + comb_ldx(kt) + 1);
+    const size_t red = (size_t)4 * mt * 2 * 32;  // cross-warp reduction of the accumulators
+    return sizeof(double) * std::max(pipe, red);
 }
 
-template <int MT, typename TP>
+template <int MT, int NST, typename TP>
 __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP* __restrict__ part, int nsplit,
                                                       const double* __restrict__ X, const double* __restrict__ pre,
                                                       const double* __restrict__ diag,
@@ -311,23 +319,23 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
                                                       const int32_t* __restrict__ col,
                                                       const double* __restrict__ val, int nb,
                                                       double* __restrict__ Y) {
-    // column stride of a staged block: MT * 8 rows + 4 (= 4 or 12 mod 16 doubles, so the
-    // four k-rows a half-warp reads fall in distinct banks)
+    // column stride of a staged block: MT * 8 rows + 4 (= 4 or 12 mod 16 doubles)
     constexpr int LDC = MT * 8 + 4;
-    constexpr int LDX = kCombLDX;
-    const int KS = (nb + 3) / 4, KP = KS * 4;
-    extern __shared__ __align__(16) double smd[];
-    double* sC = smd;                   // [2][KP][LDC], sC[q * LDC + r] = C_b[r][q]
-    double* sX = sC + 2 * KP * LDC;     // [2][KP][LDX], sX[q * LDX + cc] = X[col_b * nb + q][c0 + cc]
-    double* sP = sX + 2 * KP * LDX;     // [2][KP] preconditioner of the slab rows
-    const int P = blockIdx.x;
     const int c0 = blockIdx.y * kCombTile;
     const int kt = min(kCombTile, k - c0);
+    const int LDX = comb_ldx(kt);
+    const int KS = (nb + 3) / 4, KP = KS * 4;
+    const int SSTR = KP * (LDC + LDX + 1);  // doubles per pipeline stage
+    extern __shared__ __align__(16) double smd[];
+    // stage t: sC = smd + t SSTR ([KP][LDC], sC[q LDC + r] = C_b[r][q]),
+    //          sX = sC + KP LDC ([KP][LDX], sX[q LDX + cc] = X[col_b nb + q][c0 + cc]),
+    //          sP = sX + KP LDX ([KP] preconditioner of the slab rows)
+    const int P = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row0 = (int64_t)P * nb;
     const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
     // padding rows/columns stay zero: the copies below write only the live part
-    for (int e = threadIdx.x; e < 2 * KP * (LDC + LDX + 1); e += blockDim.x) smd[e] = 0.0;
+    for (int e = threadIdx.x; e < NST * SSTR; e += blockDim.x) smd[e] = 0.0;
     __syncthreads();
 
     const bool v16 = (nb & 1) == 0;  // 16-byte copies of block columns (the blocks are 16-byte aligned)
@@ -335,7 +343,7 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
                      (reinterpret_cast<uintptr_t>(X) & 15) == 0;
     auto issue = [&](int b, int st) {
         const double* vb = val + (int64_t)b * nb * nb;
-        double* dC = sC + st * KP * LDC;
+        double* dC = smd + st * SSTR;
         if (v16) {
             const int h = nb >> 1;
             for (int e = threadIdx.x; e < nb * h; e += blockDim.x) {
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
             }
         }
         const int64_t base = (int64_t)col[b] * nb;
-        double* dX = sX + st * KP * LDX;
+        double* dX = dC + KP * LDC;
         if (x16) {
             const int h = kt >> 1;
             for (int e = threadIdx.x; e < nb * h; e += blockDim.x) {
@@ -363,52 +371,74 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
             }
         }
         if (pre)
-            for (int q = threadIdx.x; q < nb; q += blockDim.x) cp_async8(sP + st * KP + q, pre + base + q);
-        cp_async_commit();
+            for (int q = threadIdx.x; q < nb; q += blockDim.x) cp_async8(dX + KP * LDX + q, pre + base + q);
     };
 
-    // warps to (n-tile, m-tile subset): with fewer than four n-tiles the warps share
-    // an n-tile and split its m-tiles
+    // warps to (n-tile, k-step subset): with fewer than four n-tiles the warps sharing an
+    // n-tile split the block's k-steps (each keeps all MT accumulator chains busy) and
+    // their partial sums are added through shared memory at the end
     const int ntiles = (kt + 7) / 8;
     const int nw = ntiles >= 4 ? 4 : ntiles;  // distinct n-tiles in use
-    const int mstep = 4 / nw;                 // 1, 2 or 4 (nw = 3: one warp idle)
-    const int nt = warp % nw, moff = warp / nw;
-    const bool wact = moff < mstep;
+    const int ksplit = 4 / nw;                // 1, 2 or 4 (nw = 3: one warp idle)
+    const int nt = warp % nw, kq = warp / nw;
+    const bool wact = kq < ksplit;
     double acc[MT][2];
 #pragma unroll
     for (int m = 0; m < MT; ++m) acc[m][0] = acc[m][1] = 0.0;
 
-    if (b0 < b1) issue(b0, 0);
+    // NST-stage pipeline: blocks b .. b + NST - 2 are in flight while block b is used;
+    // one (possibly empty) copy group is committed per step so the group count is uniform
+#pragma unroll
+    for (int t = 0; t < NST - 1; ++t) {
+        if (b0 + t < b1) issue(b0 + t, t);
+        cp_async_commit();
+    }
     for (int b = b0; b < b1; ++b) {
-        const int st = (b - b0) & 1;
-        if (b + 1 < b1) {
-            issue(b + 1, st ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
+        const int st = (b - b0) % NST;
+        cp_async_wait<NST - 2>();
+        __syncthreads();  // block b landed for all threads; stage (b - 1) % NST is free
+        if (b + NST - 1 < b1) issue(b + NST - 1, (b - b0 + NST - 1) % NST);
+        cp_async_commit();
         if (wact) {
-            const double* cC = sC + st * KP * LDC + (lane >> 2);
-            const double* cX = sX + st * KP * LDX + 8 * nt + (lane >> 2);
-            const double* cP = sP + st * KP;
-            for (int ks = 0; ks < KS; ++ks) {
+            const double* cC = smd + st * SSTR + (lane >> 2);
+            const double* cX = smd + st * SSTR + KP * LDC + 8 * nt + (lane >> 2);
+            const double* cP = smd + st * SSTR + KP * LDC + KP * LDX;
+            for (int ks = kq; ks < KS; ks += ksplit) {
                 const int q = 4 * ks + (lane & 3);
                 double bv = cX[q * LDX];
                 if (pre) bv *= cP[q];
 #pragma unroll
-                for (int m = 0; m < MT; ++m)
-                    if (m % mstep == moff) dmma884(acc[m][0], acc[m][1], cC[q * LDC + 8 * m], bv);
+                for (int m = 0; m < MT; ++m) dmma884(acc[m][0], acc[m][1], cC[q * LDC + 8 * m], bv);
             }
         }
-        __syncthreads();  // stage st is refilled two iterations later
+    }
+    cp_async_wait<0>();
+    if (ksplit > 1) {
+        // add the k-step partial sums of the warps sharing an n-tile (stage memory reused)
+        __syncthreads();
+        double* red = smd;  // [warp][MT][2][32]
+        if (wact && kq > 0)
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                red[((warp * MT + m) * 2 + 0) * 32 + lane] = acc[m][0];
+                red[((warp * MT + m) * 2 + 1) * 32 + lane] = acc[m][1];
+            }
+        __syncthreads();
+        if (wact && kq == 0)
+            for (int o = 1; o < ksplit; ++o) {
+                const int w2 = nt + o * nw;
+#pragma unroll
+                for (int m = 0; m < MT; ++m) {
+                    acc[m][0] += red[((w2 * MT + m) * 2 + 0) * 32 + lane];
+                    acc[m][1] += red[((w2 * MT + m) * 2 + 1) * 32 + lane];
+                }
+            }
     }
 
-    if (!wact) return;
+    if (!wact || kq > 0) return;
     const int64_t tot = n * (int64_t)k;
 #pragma unroll
     for (int m = 0; m < MT; ++m) {
-        if (m % mstep != moff) continue;
         const int r = 8 * m + (lane >> 2);
         if (r >= nb) continue;
         const int64_t i = row0 + r;

@@ -72,6 +72,9 @@ namespace bie {
 constexpr double kDeltaBF16X3 = 4e-6;
 constexpr double kDeltaBF16X6 = 3e-7;
 constexpr double kDeltaFP32 = 3e-7;
+// Fewest columns for the tensor-core direct sum (K3 pads to 16 columns; its kernel-tile
+// generation, not the MMA, bounds it, so from 8 columns on it beats the FP32 CUDA-core sum).
+constexpr int kTcMinCols = 8;
 
 namespace {
 
@@ -435,22 +438,28 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
     const int32_t* cl = corr ? g->col.as<int32_t>() : nullptr;
     const double* vl = corr ? g->val.as<double>() : nullptr;
     const int mt = (g->nb + 7) / 8;
-    if (g->nb > 0 && mt <= 8 && (int64_t)g->npanels * g->nb == g->n) {
-        const size_t sm = combine_smem_bytes(g->nb);
+    const bool panel_rows = g->nb > 0 && (int64_t)g->npanels * g->nb == g->n;
+    if (panel_rows && mt <= 8) {
+        // the block products on the FP64 tensor path, two pipeline stages
+        const int nst = 2;
+        const size_t sm = combine_smem_bytes(g->nb, std::min(k, kCombTile), nst);
         dim3 grid((unsigned)g->npanels, (unsigned)((k + kCombTile - 1) / kCombTile));
-#define BIE_COMB(MT)                                       \
-    ensure_smem_limit((const void*)k_combine_dmma<MT, TP>, sm); \
-    k_combine_dmma<MT, TP><<<grid, 128, sm, s>>>(g->n, k, part, nsplit, X, pre, dgp, rp, cl, vl, g->nb, Y)
-        switch (mt) {
-            case 1: BIE_COMB(1); break;
-            case 2: BIE_COMB(2); break;
-            case 3: BIE_COMB(3); break;
-            case 4: BIE_COMB(4); break;
-            case 5: BIE_COMB(5); break;
-            case 6: BIE_COMB(6); break;
-            case 7: BIE_COMB(7); break;
-            default: BIE_COMB(8); break;
-        }
+#define BIE_COMB(MT, NST)                                       \
+    ensure_smem_limit((const void*)k_combine_dmma<MT, NST, TP>, sm); \
+    k_combine_dmma<MT, NST, TP><<<grid, 128, sm, s>>>(g->n, k, part, nsplit, X, pre, dgp, rp, cl, vl, g->nb, Y)
+#define BIE_COMB_MT(NST)                      \
+    switch (mt) {                             \
+        case 1: BIE_COMB(1, NST); break;      \
+        case 2: BIE_COMB(2, NST); break;      \
+        case 3: BIE_COMB(3, NST); break;      \
+        case 4: BIE_COMB(4, NST); break;      \
+        case 5: BIE_COMB(5, NST); break;      \
+        case 6: BIE_COMB(6, NST); break;      \
+        case 7: BIE_COMB(7, NST); break;      \
+        default: BIE_COMB(8, NST); break;     \
+    }
+        BIE_COMB_MT(2)
+#undef BIE_COMB_MT
 #undef BIE_COMB
     } else {
         k_combine<TP><<<grid1(g->n * k), 256, 0, s>>>(g->n, k, part, nsplit, X, k, pre, dgp, rp, cl, vl, g->nb, Y, k);
@@ -462,11 +471,11 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
 void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
               cudaStream_t s) {
     Split sp;
-    const bool tc = (prec == BIE_BF16X3 || prec == BIE_BF16X6) && k >= 16;
+    const bool tc = (prec == BIE_BF16X3 || prec == BIE_BF16X6) && k >= kTcMinCols;
     if (tc) {
         sp = direct_sum_tc(g, X, k, pre, prec == BIE_BF16X6 ? 3 : 2, s);
     } else {
-        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // tensor-core precisions with k < 16 run FP32
+        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // tensor-core precisions with k < kTcMinCols run FP32
         sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
     }
     const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
@@ -1082,7 +1091,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
         // delta * ||A d|| ~ delta * ||r||, delta being the operator's relative error,
         // which is admitted only while it stays below half the tolerance.
         // Candidate operators for the residual update, cheapest first.
-        const bool tc_ok = k >= 16;
+        const bool tc_ok = k >= kTcMinCols;
         struct Upd { int prec; double delta; };
         std::vector<Upd> upd;
         if (o.precision == BIE_BF16X3 && tc_ok) upd.push_back({BIE_BF16X3, kDeltaBF16X3});
