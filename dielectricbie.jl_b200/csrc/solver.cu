@@ -1098,6 +1098,9 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
         if ((o.precision == BIE_BF16X3 || o.precision == BIE_BF16X6) && tc_ok) upd.push_back({BIE_BF16X6, kDeltaBF16X6});
         upd.push_back({BIE_FP32, kDeltaFP32});
         std::vector<double> rn = fn, eps_in(k);
+        const double inner_delta = (o.precision == BIE_BF16X3 && tc_ok)   ? kDeltaBF16X3
+                                   : (o.precision == BIE_BF16X6 && tc_ok) ? kDeltaBF16X6
+                                                                          : kDeltaFP32;
         BIE_CK(cudaMemcpyAsync(rbuf, dF, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
         have_true_resid = true;
         for (int it_out = 0;; ++it_out) {
@@ -1126,7 +1129,11 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
                 break;
             }
             if (it_out >= o.max_outer || iters >= o.itmax) break;
-            for (int c = 0; c < k; ++c) eps_in[c] = std::max(o.inner_rtol * rn[c], 0.5 * tol[c]);
+            // inner tolerance: inner_rtol |r|, but not below half the outer tolerance nor
+            // below twice the inner operator's own relative error (iterating past that
+            // cannot lower the true residual of this pass)
+            for (int c = 0; c < k; ++c)
+                eps_in[c] = std::max({o.inner_rtol * rn[c], 0.5 * tol[c], 2.0 * inner_delta * rn[c]});
             GmresResult r = gmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
                                   o.itmax - iters, o.restart, o.check_every, s);
             iters += r.iters;

@@ -199,7 +199,8 @@ typedef struct {
     int itmax;           /* maximum Krylov iterations in total (default 500) */
     int restart;         /* Krylov basis capacity before restart (default 200) */
     int precision;       /* bie_precision of the Krylov operator (default BIE_FP64) */
-    double inner_rtol;   /* mixed precision: relative tolerance of each inner solve (default 1e-6) */
+    double inner_rtol;   /* mixed precision: relative tolerance of each inner solve (default 1e-6; never
+                            tighter than twice the inner operator's relative error) */
     int max_outer;       /* mixed precision: maximum refinement steps (default 8) */
     int precondition;    /* right diagonal preconditioner 1/t_P (src/solver/multi_rhs.jl:234-247) */
     int check_every;     /* host convergence check period in iterations (default 1) */
