@@ -311,6 +311,9 @@ inline size_t combine_smem_bytes(int nb, int kt, int stages) {
     return sizeof(double) * std::max(pipe, red);
 }
 
+// With gsum != nullptr the panel's block list is split into groups of bpg blocks
+// (blockIdx.z = group) and each group writes its block sum to gsum[z][i][c]; the
+// reduction over groups, split partials and diagonal is then k_combine_groups.
 template <int MT, int NST, typename TP>
 __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP* __restrict__ part, int nsplit,
                                                       const double* __restrict__ X, const double* __restrict__ pre,
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
                                                       const int32_t* __restrict__ rowptr,
                                                       const int32_t* __restrict__ col,
                                                       const double* __restrict__ val, int nb,
-                                                      double* __restrict__ Y) {
+                                                      double* __restrict__ Y, int bpg, double* __restrict__ gsum) {
     // column stride of a staged block: MT * 8 rows + 4 (= 4 or 12 mod 16 doubles)
     constexpr int LDC = MT * 8 + 4;
     const int c0 = blockIdx.y * kCombTile;
@@ -333,7 +336,11 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
     const int P = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row0 = (int64_t)P * nb;
-    const int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
+    int b0 = val ? rowptr[P] : 0, b1 = val ? rowptr[P + 1] : 0;
+    if (gsum) {
+        b0 += (int)blockIdx.z * bpg;
+        b1 = min(b1, b0 + bpg);
+    }
     // padding rows/columns stay zero: the copies below write only the live part
     for (int e = threadIdx.x; e < NST * SSTR; e += blockDim.x) smd[e] = 0.0;
     __syncthreads();
@@ -448,12 +455,37 @@ __global__ void __launch_bounds__(128) k_combine_dmma(int64_t n, int k, const TP
             const int c = c0 + 8 * nt + 2 * (lane & 3) + h;
             if (c >= c0 + kt) continue;
             const int64_t e = i * k + c;
+            if (gsum) {
+                gsum[(int64_t)blockIdx.z * tot + e] = acc[m][h];
+                continue;
+            }
             double sp = 0.0;
             for (int p = 0; p < nsplit; ++p) sp += (double)part[(int64_t)p * tot + e];
             double y = sp * kInv4Pi + acc[m][h];
             if (diag) y += dgi * X[e];
             Y[e] = y;
         }
+    }
+}
+
+// Y[e] = sum_z gsum[z][e] + (1/4pi) sum_s part[s][e] + t_i p_i X[e], e = i k + c.
+template <typename TP>
+__global__ void k_combine_groups(int64_t n, int k, const double* __restrict__ gsum, int ngroups,
+                                 const TP* __restrict__ part, int nsplit, const double* __restrict__ X,
+                                 const double* __restrict__ pre, const double* __restrict__ diag,
+                                 double* __restrict__ Y) {
+    const int64_t tot = n * (int64_t)k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        double a = 0.0;
+        for (int z = 0; z < ngroups; ++z) a += gsum[(int64_t)z * tot + e];
+        double sp = 0.0;
+        for (int p = 0; p < nsplit; ++p) sp += (double)part[(int64_t)p * tot + e];
+        double y = sp * kInv4Pi + a;
+        if (diag) {
+            const int64_t i = e / k;
+            y += diag[i] * (pre ? pre[i] : 1.0) * X[e];
+        }
+        Y[e] = y;
     }
 }
 

@@ -29,7 +29,8 @@ struct bie_geom {
     bie::Buf x, y, z, nx, ny, nz, w, diag, pinv, perm;
     bie::Buf rowptr, col, val;
     // operator workspace
-    bie::Buf part, small, bpack, errflag;
+    bie::Buf part, small, bpack, errflag, cpart;
+    int max_row_blocks = 0;  // longest BSR block row (blocks of one target panel)
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -443,10 +444,27 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
         // the block products on the FP64 tensor path, two pipeline stages
         const int nst = 2;
         const size_t sm = combine_smem_bytes(g->nb, std::min(k, kCombTile), nst);
-        dim3 grid((unsigned)g->npanels, (unsigned)((k + kCombTile - 1) / kCombTile));
+        const int64_t ctas = (int64_t)g->npanels * ((k + kCombTile - 1) / kCombTile);
+        // long block rows of few panels: split each row into groups of blocks so that
+        // about 8 CTAs per SM run (summed by k_combine_groups)
+        int ngroups = 1, bpg = 0;
+        if (vl && g->max_row_blocks > 8) {
+            const int64_t want = (8 * (int64_t)g->sms + ctas - 1) / ctas;
+            ngroups = (int)std::min<int64_t>(want, (g->max_row_blocks + 3) / 4);
+            ngroups = std::max(ngroups, 1);
+            bpg = (g->max_row_blocks + ngroups - 1) / ngroups;
+            ngroups = (g->max_row_blocks + bpg - 1) / bpg;
+        }
+        double* gsum = nullptr;
+        if (ngroups > 1) {
+            g->cpart.ensure(sizeof(double) * (size_t)ngroups * g->n * k);
+            gsum = g->cpart.as<double>();
+        }
+        dim3 grid((unsigned)g->npanels, (unsigned)((k + kCombTile - 1) / kCombTile), (unsigned)ngroups);
 #define BIE_COMB(MT, NST)                                       \
     ensure_smem_limit((const void*)k_combine_dmma<MT, NST, TP>, sm); \
-    k_combine_dmma<MT, NST, TP><<<grid, 128, sm, s>>>(g->n, k, part, nsplit, X, pre, dgp, rp, cl, vl, g->nb, Y)
+    k_combine_dmma<MT, NST, TP><<<grid, 128, sm, s>>>(g->n, k, part, nsplit, X, pre, dgp, rp, cl, vl, g->nb, Y, bpg, \
+                                                      gsum)
 #define BIE_COMB_MT(NST)                      \
     switch (mt) {                             \
         case 1: BIE_COMB(1, NST); break;      \
@@ -461,6 +479,12 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
         BIE_COMB_MT(2)
 #undef BIE_COMB_MT
 #undef BIE_COMB
+        if (gsum) {
+            BIE_CK(cudaGetLastError());
+            const int64_t tot = g->n * (int64_t)k;
+            const unsigned blocks = (unsigned)std::min<int64_t>((tot + 255) / 256, (int64_t)g->sms * 8);
+            k_combine_groups<TP><<<blocks, 256, 0, s>>>(g->n, k, gsum, ngroups, part, nsplit, X, pre, dgp, Y);
+        }
     } else {
         k_combine<TP><<<grid1(g->n * k), 256, 0, s>>>(g->n, k, part, nsplit, X, k, pre, dgp, rp, cl, vl, g->nb, Y, k);
     }
@@ -611,7 +635,7 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             h *= 1099511628211ull;
         };
         mix((uint64_t)k); mix((uint64_t)prec); mix(flags); mix((uint64_t)m); mix((uintptr_t)pre);
-        const bie::Buf* bufs[] = {&g->V, &g->W, &g->part, &g->bpack, &g->dpart, &g->h, &g->h2, &g->hn, &g->R,
+        const bie::Buf* bufs[] = {&g->V, &g->W, &g->part, &g->bpack, &g->cpart, &g->dpart, &g->h, &g->h2, &g->hn, &g->R,
                                   &g->cs, &g->sn, &g->gv, &g->active, &g->jlast, &g->eps, &g->resid, &g->errflag};
         for (const auto* b : bufs) {
             mix((uintptr_t)b->p);
@@ -861,6 +885,7 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
     upload(g->pinv, col3.data(), n, s);
     if (nblocks > 0) {
         upload(g->rowptr, rowptr, (size_t)npanels + 1, s);
+        for (int32_t p = 0; p < npanels; ++p) g->max_row_blocks = std::max(g->max_row_blocks, rowptr[p + 1] - rowptr[p]);
         upload(g->col, col, nblocks, s);
         upload(g->val, val, (size_t)nblocks * nb * nb, s);
     }
@@ -885,7 +910,7 @@ void geom_destroy(bie_geom* g) {
         DeviceGuard dg(g->device);
         if (g->stream) cudaStreamSynchronize(g->stream);
         bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->perm, &g->rowptr,
-                           &g->col, &g->val, &g->part, &g->small, &g->bpack, &g->errflag, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
+                           &g->col, &g->val, &g->part, &g->small, &g->bpack, &g->errflag, &g->cpart, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
                            &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
         for (auto* b : all) b->release();
