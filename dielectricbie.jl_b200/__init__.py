@@ -190,11 +190,16 @@ class DielectricInterface:
 
     # cached near-field blocks and device geometries ----------------------------
     def near(self, max_order=8, up_tol=1e-9, correct_edges=True, adaptive: Optional[AdaptiveConfig] = None,
-             nthreads=0) -> "_Near":
+             nthreads=0, setup_device: Optional[int] = None) -> "_Near":
+        """Near-field corrections (cached). setup_device: CUDA device for the adaptive blocks'
+        moment sums (bitwise equal to the host's); None = device 0 when the library sees a
+        CUDA device, else the host."""
+        if setup_device is None:
+            setup_device = 0 if _abi.device_count() > 0 else -1
         ad = adaptive or AdaptiveConfig(atol=up_tol)
         key = (int(max_order), float(up_tol), bool(correct_edges), ad, int(nthreads))
         if key not in self._near:
-            self._near[key] = _Near(self, max_order, up_tol, correct_edges, ad, nthreads)
+            self._near[key] = _Near(self, max_order, up_tol, correct_edges, ad, nthreads, setup_device)
         return self._near[key]
 
     def geom(self, near: Optional["_Near"], device: int = 0) -> "_Geom":
@@ -267,12 +272,13 @@ def laplace3d_grad(src, trg, n) -> float:
 # Near field (src/kernel/laplace3d_near.jl:240-392, laplace3d_near_upsampling.jl:127-276)
 # ---------------------------------------------------------------------------
 class _Near:
-    def __init__(self, itf, max_order, up_tol, correct_edges, ad: AdaptiveConfig, nthreads):
+    def __init__(self, itf, max_order, up_tol, correct_edges, ad: AdaptiveConfig, nthreads, setup_device=-1):
         o = _abi.NearOpts()
         lib().bie_near_opts_default(C.byref(o))
         o.max_order, o.up_tol, o.correct_edges = int(max_order), float(up_tol), int(bool(correct_edges))
         o.adaptive_atol, o.adaptive_rtol = float(ad.atol), float(ad.rtol)
         o.adaptive_n_GL, o.adaptive_max_depth, o.nthreads = int(ad.n_GL), int(ad.max_depth), int(nthreads)
+        o.device = int(setup_device)
         h = C.c_void_p()
         check(lib().bie_near_build(itf._h, C.byref(o), C.byref(h)))
         self._h = h

@@ -45,7 +45,7 @@ class NotConverged(BieError):
 class NearOpts(C.Structure):
     _fields_ = [("max_order", C.c_int), ("up_tol", C.c_double), ("correct_edges", C.c_int),
                 ("adaptive_atol", C.c_double), ("adaptive_rtol", C.c_double), ("adaptive_n_GL", C.c_int),
-                ("adaptive_max_depth", C.c_int), ("nthreads", C.c_int)]
+                ("adaptive_max_depth", C.c_int), ("nthreads", C.c_int), ("device", C.c_int)]
 
 
 class SolveOpts(C.Structure):

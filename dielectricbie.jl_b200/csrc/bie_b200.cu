@@ -243,6 +243,7 @@ void bie_near_opts_default(bie_near_opts* o) {
     o->adaptive_n_GL = d.adaptive_n_GL;
     o->adaptive_max_depth = d.adaptive_max_depth;
     o->nthreads = d.nthreads;
+    o->device = d.device;
 }
 
 int bie_near_build(const bie_mesh* m, const bie_near_opts* o, bie_near** out) {
@@ -258,6 +259,7 @@ int bie_near_build(const bie_mesh* m, const bie_near_opts* o, bie_near** out) {
             no.adaptive_n_GL = o->adaptive_n_GL;
             no.adaptive_max_depth = o->adaptive_max_depth;
             no.nthreads = o->nthreads;
+            no.device = o->device;
         }
         auto h = std::make_unique<bie_near>();
         std::string err;

@@ -5,6 +5,9 @@
 #include "host_setup.h"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <array>
 #include <cfloat>
 #include <climits>
@@ -745,6 +748,7 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
     for (int p = 0; p < P; ++p) std::copy(m.corners.begin() + 12 * p, m.corners.begin() + 12 * p + 12, cpts.begin() + 12 * p);
     if (P > 0) cgrid.build(cpts.data(), 4 * (int64_t)P, std::max(Lmax / 4, 1e-12));
 
+    const auto t_start = std::chrono::steady_clock::now();
     const double log_atol = std::log(o.up_tol);
     std::vector<std::vector<std::pair<int, int>>> ups(P);  // per source: (target, p_up)
     std::vector<std::vector<int>> adp(P);
@@ -803,17 +807,26 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
         for (int j : adp[i]) { out.adp_i.push_back(i); out.adp_j.push_back(j); }
     }
 
+    const auto t_list = std::chrono::steady_clock::now();
+    double t_ups = 0.0, t_adp = 0.0, t_walk = 0.0;  // thread-seconds per block kind (BIE_TRACE)
+    int64_t n_leaves = 0;
     // Blocks, computed per source panel (one upsampling order per source: the max
     // over its upsample neighbours, laplace3d_near_upsampling.jl:164-183).
     struct Blk { int row, col; std::vector<double> v; };
     std::vector<std::vector<Blk>> per_src(P);
+    // adaptive pairs whose moment sums run on the GPU: (target, leaves) per source
+    const bool gpu_adp = o.device >= 0 && nq <= 6;
+    struct AdpJob { int j; std::vector<std::array<double, 4>> leaves; };
+    std::vector<std::vector<AdpJob>> adp_jobs(gpu_adp ? P : 0);
+    const int nGL = o.adaptive_n_GL == 0 ? nq : o.adaptive_n_GL;
     int hit_any = 0;
     const double aatol = o.adaptive_atol < 0 ? o.up_tol : o.adaptive_atol;
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nth) reduction(| : hit_any)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nth) reduction(| : hit_any) reduction(+ : t_ups, t_adp, t_walk, n_leaves)
 #endif
     for (int i = 0; i < P; ++i) {
         if (ups[i].empty() && adp[i].empty()) continue;
+        const auto t0 = std::chrono::steady_clock::now();
         std::vector<double> Kb((size_t)np * np), Kd((size_t)np * np), kmat;
         auto emit = [&](int j) {
             Blk b{j, i, std::vector<double>((size_t)np * np)};
@@ -832,6 +845,8 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
                 emit(e.first);
             }
         }
+        const auto t1 = std::chrono::steady_clock::now();
+        t_ups += std::chrono::duration<double>(t1 - t0).count();
         for (int j : adp[i]) {
             Adaptive A;
             A.m = &m; A.f = fr[i];
@@ -847,14 +862,72 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
                 double d = norm(ld(m.pts.data() + 3 * ((size_t)j * np + t)) - c1);
                 if (d < best) { best = d; rep = t; }
             }
+            const auto tw = std::chrono::steady_clock::now();
             A.walk(ld(m.pts.data() + 3 * ((size_t)j * np + rep)), ld(m.normals.data() + 3 * j), -1, 1, -1, 1, 0);
+            t_walk += std::chrono::duration<double>(std::chrono::steady_clock::now() - tw).count();
+            n_leaves += (int64_t)A.leaves.size();
             if (A.hit) hit_any = 1;
+            if (gpu_adp) {
+                adp_jobs[i].push_back({j, std::move(A.leaves)});
+                continue;
+            }
             A.block(j, Kb.data());
             direct_block(m, i, j, Kd.data());
             emit(j);
         }
+        t_adp += std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+    }
+    if (gpu_adp) {
+        // one launch for every adaptive pair, then the direct blocks and the differences
+        std::vector<int> trg;
+        std::vector<double> frames, leaves;
+        std::vector<int64_t> off{0};
+        for (int i = 0; i < P; ++i)
+            for (auto& jb : adp_jobs[i]) {
+                trg.push_back(jb.j);
+                const PanelFrame& f = fr[i];
+                const double fv[10] = {f.cc.x, f.cc.y, f.cc.z, f.bma.x, f.bma.y, f.bma.z,
+                                       f.dma.x, f.dma.y, f.dma.z, f.scale};
+                frames.insert(frames.end(), fv, fv + 10);
+                for (auto& L : jb.leaves) leaves.insert(leaves.end(), L.begin(), L.end());
+                off.push_back((int64_t)leaves.size() / 4);
+            }
+        const int npairs = (int)trg.size();
+        std::vector<double> Kball((size_t)npairs * np * np);
+        std::vector<double> xg(nGL), wg(nGL);
+        gauss_legendre(nGL, xg.data(), wg.data());
+        if (adaptive_blocks_gpu(o.device, nq, nGL, m.glx.data(), m.bary.data(), xg.data(), wg.data(), m.pts.data(),
+                                N, m.normals.data(), P, npairs, trg.data(), frames.data(), off.data(), leaves.data(),
+                                Kball.data(), err) != 0)
+            return -1;
+        std::vector<int64_t> first(P + 1, 0);
+        for (int i = 0; i < P; ++i) first[i + 1] = first[i] + (int64_t)adp_jobs[i].size();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nth)
+#endif
+        for (int i = 0; i < P; ++i) {
+            std::vector<double> Kd((size_t)np * np);
+            for (size_t q = 0; q < adp_jobs[i].size(); ++q) {
+                const int j = adp_jobs[i][q].j;
+                const double* Kb = Kball.data() + (size_t)(first[i] + (int64_t)q) * np * np;
+                direct_block(m, i, j, Kd.data());
+                Blk b{j, i, std::vector<double>((size_t)np * np)};
+                for (int s = 0; s < np; ++s)
+                    for (int r = 0; r < np; ++r) b.v[(size_t)s * np + r] = Kb[(size_t)r * np + s] - Kd[(size_t)r * np + s];
+                per_src[i].push_back(std::move(b));
+            }
+        }
     }
     out.hit_max = hit_any;
+    if (std::getenv("BIE_TRACE")) {
+        const double dl = std::chrono::duration<double>(t_list - t_start).count();
+        const double db = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_list).count();
+        std::fprintf(stderr,
+                     "[bie] near_build: %d panels, neighbour lists %.3f s, blocks %.3f s (thread-seconds: "
+                     "upsampled %.3f, adaptive %.3f of which tree walks %.3f; %zu upsampled and %zu adaptive pairs, "
+                     "%lld leaves)\n",
+                     P, dl, db, t_ups, t_adp, t_walk, out.ups_i.size(), out.adp_i.size(), (long long)n_leaves);
+    }
     // assemble BSR (rows = target panels), columns sorted within each row
     std::vector<std::vector<std::pair<int, const Blk*>>> rows(P);
     for (int i = 0; i < P; ++i)

@@ -48,7 +48,18 @@ struct NearOpts {
     int adaptive_n_GL = 0;
     int adaptive_max_depth = 20;
     int nthreads = 0;
+    int device = -1;  // >= 0: the adaptive blocks' moment sums run on this CUDA device (n_quad <= 6)
 };
+
+// Moment blocks of the adaptive (touching) pairs on a CUDA device (near_gpu.cu):
+// pair p has target panel trg[p], source frame frames[10 p ..] = (cc, b - a, d - a, scale)
+// and the quadtree leaves leaves[4 l ..], l in [leaf_off[p], leaf_off[p + 1]); Kb receives
+// npairs x (nq^2 x nq^2) blocks in the host's layout, bitwise equal to the host sums.
+// Returns 0, or -1 with err set.
+int adaptive_blocks_gpu(int device, int nq, int ngl, const double* glx, const double* bary, const double* xg,
+                        const double* wg, const double* pts, int64_t npts, const double* normals, int npanels,
+                        int npairs, const int* trg, const double* frames, const int64_t* leaf_off,
+                        const double* leaves, double* Kb, std::string& err);
 
 // Near-field corrections in block-sparse-row form: block rows = target panels,
 // block columns = source panels, each block nb x nb (nb = nq^2) stored
