@@ -484,6 +484,7 @@ def main():
     ap.add_argument("--profile-matvec", action="store_true",
                     help="apply the refined and the FP64 operator once each to k columns and exit "
                          "(small case for ncu captures)")
+    ap.add_argument("--columns", type=int, default=0, help="--profile-matvec: columns (default: the workload's k)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -518,6 +519,7 @@ def main():
     g = op.geom._h
     n, k = itf.n, wl["k"]
     if args.profile_matvec:
+        k = args.columns or k
         X = np.asfortranarray(np.random.default_rng(0).standard_normal((n, k)))
         op.mul(X, precision=args.precision)
         op.mul(X, precision="fp64")

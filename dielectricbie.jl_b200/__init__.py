@@ -367,7 +367,7 @@ class GPUDielectricOperator:
     accept (size, eltype, mul!; src/solver/multi_rhs.jl:46-141), with the FMM
     replaced by the exact direct sum. ``precision`` selects the arithmetic of the
     direct sum: "fp64" (plain), "fp32" (FP64 tile partials) or "bf16x3"
-    (tensor-core RHS contraction, k >= 8). Corrections and diagonal stay FP64."""
+    (tensor-core RHS contraction; FP32 CUDA-core sum for k = 1, 2, 4). Corrections and diagonal stay FP64."""
 
     def __init__(self, interface: DielectricInterface, *, precision: str = "fp64", corrections: bool = True,
                  up_tol: float = 1e-9, max_order: int = 8, correct_edges: bool = True,

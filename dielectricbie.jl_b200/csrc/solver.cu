@@ -73,9 +73,12 @@ namespace bie {
 constexpr double kDeltaBF16X3 = 4e-6;
 constexpr double kDeltaBF16X6 = 3e-7;
 constexpr double kDeltaFP32 = 3e-7;
-// Fewest columns for the tensor-core direct sum (K3 pads to 16 columns; its kernel-tile
-// generation, not the MMA, bounds it, so from 8 columns on it beats the FP32 CUDA-core sum).
-constexpr int kTcMinCols = 8;
+// Split-BF16 precisions run the tensor-core direct sum (K3, padded to 16 columns and
+// bound by its kernel-tile generation, so its time hardly depends on k) unless the FP32
+// CUDA-core sum (K2) covers k in one pass (k = 1, 2, 4), which is faster there.
+inline bool use_tc(int prec, int k) {
+    return (prec == BIE_BF16X3 || prec == BIE_BF16X6) && !(k == 1 || k == 2 || k == 4);
+}
 
 namespace {
 
@@ -495,11 +498,11 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
 void apply_op(bie_geom* g, const double* X, double* Y, int k, int prec, uint32_t flags, const double* pre,
               cudaStream_t s) {
     Split sp;
-    const bool tc = (prec == BIE_BF16X3 || prec == BIE_BF16X6) && k >= kTcMinCols;
+    const bool tc = use_tc(prec, k);
     if (tc) {
         sp = direct_sum_tc(g, X, k, pre, prec == BIE_BF16X6 ? 3 : 2, s);
     } else {
-        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // tensor-core precisions with k < kTcMinCols run FP32
+        Kern kind = prec == BIE_FP64 ? Kern::DT64 : Kern::DT32;  // split-BF16 with k = 1, 2, 4 runs K2 (FP32)
         sp = direct_sum(g, kind, X, k, k, pre, nullptr, 0, s);
     }
     const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
@@ -1116,7 +1119,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
         // delta * ||A d|| ~ delta * ||r||, delta being the operator's relative error,
         // which is admitted only while it stays below half the tolerance.
         // Candidate operators for the residual update, cheapest first.
-        const bool tc_ok = k >= kTcMinCols;
+        const bool tc_ok = use_tc(o.precision == BIE_BF16X6 ? BIE_BF16X6 : BIE_BF16X3, k);
         struct Upd { int prec; double delta; };
         std::vector<Upd> upd;
         if (o.precision == BIE_BF16X3 && tc_ok) upd.push_back({BIE_BF16X3, kDeltaBF16X3});

@@ -44,9 +44,9 @@ typedef enum {
 typedef enum {
     BIE_FP64 = 0,   /* plain: FP64 end to end */
     BIE_FP32 = 1,   /* FP32 direct sum (FP64 tile partials), FP64 corrections/diag */
-    BIE_BF16X3 = 2, /* split-BF16 three-term tensor-core RHS contraction (k >= 8),
+    BIE_BF16X3 = 2, /* split-BF16 three-term tensor-core RHS contraction (FP32 sum for k = 1, 2, 4),
                        FP32 kernel tiles, FP64 corrections/diag */
-    BIE_BF16X6 = 3  /* three bf16 pieces per operand, six tensor-core products (k >= 8):
+    BIE_BF16X6 = 3  /* three bf16 pieces per operand, six tensor-core products (idem):
                        about FP32 accuracy; the refinement's residual updates use it */
 } bie_precision;
 
