@@ -99,21 +99,43 @@ template <int C>
 __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restrict__ X, int ldx, int c0,
                                                   const double* __restrict__ pre, int64_t chunk,
                                                   double* __restrict__ part, int ldp) {
-    extern __shared__ float smf[];
+    // Source pairs (t, t + 1) run as packed f32x2 operations. Staged tiles are padded to
+    // kTS sources with far-away coordinates and zero values, so pairs never straddle
+    // the tile end.
+    extern __shared__ __align__(16) float smf[];
     float* sx = smf;
     float* sy = sx + kTS;
     float* sz = sy + kTS;
-    float* sq = sz + kTS;  // [kTS][C]
+    float* sq = sz + kTS;  // [C][kTS]: column c of the tile's sources, contiguous
     const int64_t i0 = (int64_t)blockIdx.x * kTB;
     const bool valid = i0 + threadIdx.x < g.n;
     const int64_t i = valid ? (int64_t)g.perm[i0 + threadIdx.x] : g.n;  // original index of the target
     const int64_t io = g.perm[min(i0, g.n - 1)];
     const double ox = g.x[io], oy = g.y[io], oz = g.z[io];
-    float xi = 0.f, yi = 0.f, zi = 0.f, n0 = 0.f, n1 = 0.f, n2 = 0.f;
+    float xi = -1.0e18f, yi = -1.0e18f, zi = -1.0e18f, n0 = 0.f, n1 = 0.f, n2 = 0.f;
     if (valid) {
         xi = (float)(g.x[i] - ox); yi = (float)(g.y[i] - oy); zi = (float)(g.z[i] - oz);
         n0 = (float)g.nx[i]; n1 = (float)g.ny[i]; n2 = (float)g.nz[i];
     }
+    // warp-uniform normal axis: n.(x - y) is then the signed axis difference, the sign
+    // applied to the output
+    int code = 3;
+    float sgn = 1.f;
+    if (fabsf(n0) == 1.f && n1 == 0.f && n2 == 0.f) { code = 0; sgn = n0; }
+    else if (fabsf(n1) == 1.f && n0 == 0.f && n2 == 0.f) { code = 1; sgn = n1; }
+    else if (fabsf(n2) == 1.f && n0 == 0.f && n1 == 0.f) { code = 2; sgn = n2; }
+    const int cmin = __reduce_min_sync(0xFFFFFFFFu, valid ? code : 4);
+    const int cmax = __reduce_max_sync(0xFFFFFFFFu, valid ? code : -1);
+    const int ax = (cmin == cmax && cmin < 3) ? cmin : 3;
+    if (ax == 3) sgn = 1.f;
+    const float tc[3] = {xi, yi, zi};
+    const int a1 = ax < 3 ? ax : 0, a2 = a1 == 2 ? 0 : a1 + 1, a3 = a2 == 2 ? 0 : a2 + 1;
+    const float* sA = a1 == 0 ? sx : (a1 == 1 ? sy : sz);
+    const float* sB = a2 == 0 ? sx : (a2 == 1 ? sy : sz);
+    const float* sC = a3 == 0 ? sx : (a3 == 1 ? sy : sz);
+    const uint64_t tA = pk2(tc[a1], tc[a1]), tB = pk2(tc[a2], tc[a2]), tCc = pk2(tc[a3], tc[a3]);
+    const uint64_t nA = pk2(n0, n0), nB = pk2(n1, n1), nC = pk2(n2, n2);
+    const uint64_t tiny = pk2(1e-24f, 1e-24f);  // keeps the self pair's r^-3 finite: it contributes 0
     double acc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) acc[c] = 0.0;
@@ -122,38 +144,63 @@ __global__ void __launch_bounds__(kTB) k_dt_f32(GeomDev g, const double* __restr
     for (int64_t jt = j0; jt < j1; jt += kTS) {
         const int cnt = (int)min((int64_t)kTS, j1 - jt);
         __syncthreads();
-        for (int t = threadIdx.x; t < cnt; t += kTB) {
-            const int64_t j = jt + t;
-            sx[t] = (float)(g.x[j] - ox); sy[t] = (float)(g.y[j] - oy); sz[t] = (float)(g.z[j] - oz);
-            double wj = g.w[j] * (pre ? pre[j] : 1.0);
-            const double* xr = X + j * ldx + c0;
+        for (int t = threadIdx.x; t < kTS; t += kTB) {
+            if (t < cnt) {
+                const int64_t j = jt + t;
+                sx[t] = (float)(g.x[j] - ox); sy[t] = (float)(g.y[j] - oy); sz[t] = (float)(g.z[j] - oz);
+                const double wj = g.w[j] * (pre ? pre[j] : 1.0);
+                const double* xr = X + j * ldx + c0;
 #pragma unroll
-            for (int c = 0; c < C; ++c) sq[t * C + c] = (float)(wj * xr[c]);
+                for (int c = 0; c < C; ++c) sq[c * kTS + t] = (float)(wj * xr[c]);
+            } else {
+                sx[t] = sy[t] = sz[t] = 1.0e18f;
+#pragma unroll
+                for (int c = 0; c < C; ++c) sq[c * kTS + t] = 0.f;
+            }
         }
         __syncthreads();
-        float a32[C];
+        uint64_t a2c[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) a32[c] = 0.f;
-        // The target's own node, if in this tile, has dx = dy = dz = 0 exactly (same
-        // FP64 value, same origin, same rounding); clamping r^2 keeps its r^-3 finite
-        // so it contributes exactly 0 (j != i exclusion without a branch).
+        for (int c = 0; c < C; ++c) a2c[c] = 0ull;
+        const int cnt2 = (cnt + 1) & ~1;
+        if (ax < 3) {
 #pragma unroll 4
-        for (int t = 0; t < cnt; ++t) {
-            float dx = xi - sx[t], dy = yi - sy[t], dz = zi - sz[t];
-            float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-24f);
-            float ri = rsqrt_approx(r2);
-            float nd = fmaf(n0, dx, fmaf(n1, dy, n2 * dz));
-            float gk = (nd * ri) * (ri * ri);
+            for (int t = 0; t < cnt2; t += 2) {
+                const uint64_t da = sub2(tA, *reinterpret_cast<const uint64_t*>(sA + t));
+                const uint64_t db = sub2(tB, *reinterpret_cast<const uint64_t*>(sB + t));
+                const uint64_t dc = sub2(tCc, *reinterpret_cast<const uint64_t*>(sC + t));
+                const float2 r2 = upk2(fma2(da, da, fma2(db, db, fma2(dc, dc, tiny))));
+                const uint64_t ri = pk2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                const uint64_t gk = mul2(mul2(da, ri), mul2(ri, ri));
 #pragma unroll
-            for (int c = 0; c < C; ++c) a32[c] = fmaf(gk, sq[t * C + c], a32[c]);
+                for (int c = 0; c < C; ++c)
+                    a2c[c] = fma2(gk, *reinterpret_cast<const uint64_t*>(sq + c * kTS + t), a2c[c]);
+            }
+        } else {
+#pragma unroll 4
+            for (int t = 0; t < cnt2; t += 2) {
+                const uint64_t dx = sub2(tA, *reinterpret_cast<const uint64_t*>(sx + t));
+                const uint64_t dy = sub2(tB, *reinterpret_cast<const uint64_t*>(sy + t));
+                const uint64_t dz = sub2(tCc, *reinterpret_cast<const uint64_t*>(sz + t));
+                const float2 r2 = upk2(fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, tiny))));
+                const uint64_t ri = pk2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                const uint64_t nd = fma2(nA, dx, fma2(nB, dy, mul2(nC, dz)));
+                const uint64_t gk = mul2(mul2(nd, ri), mul2(ri, ri));
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    a2c[c] = fma2(gk, *reinterpret_cast<const uint64_t*>(sq + c * kTS + t), a2c[c]);
+            }
         }
 #pragma unroll
-        for (int c = 0; c < C; ++c) acc[c] += (double)a32[c];
+        for (int c = 0; c < C; ++c) {
+            const float2 s2 = upk2(a2c[c]);
+            acc[c] += (double)s2.x + (double)s2.y;
+        }
     }
     if (valid) {
         double* o = part + ((int64_t)blockIdx.y * g.n + i) * ldp + c0;
 #pragma unroll
-        for (int c = 0; c < C; ++c) o[c] = acc[c];
+        for (int c = 0; c < C; ++c) o[c] = (double)sgn * acc[c];
     }
 }
 
