@@ -471,6 +471,32 @@ def workload_config(name, wl, n):
             "max_order": wl["max_order"], "l2": "flushed between steps (256 MB write)"}
 
 
+def run_peaks(L, device):
+    """Arithmetic ceilings of the direct sums on this device, three probe rounds each
+    (the best kept), with the SM clock sampled meanwhile; per-SM-per-clock rates use the
+    median sampled clock."""
+    import ctypes as C
+    import torch
+    names = ["fp32_fma", "fp32x2_fma", "mufu_rsqrt", "fp64_fma", "fp64_mma_m8n8k4"]
+    units = ["lane-FMA/s", "lane-FMA/s", "lane-op/s", "lane-FMA/s", "flop/s"]
+    best = {}
+    with ClockSampler(device) as clk:
+        for _ in range(3):
+            for w, nm in enumerate(names):
+                ps, ms = C.c_double(), C.c_double()
+                rc = L.bie_peak_probe(device, w, C.byref(ps), C.byref(ms))
+                if rc != 0:
+                    raise RuntimeError(f"bie_peak_probe({w}) failed: {rc}")
+                best[nm] = max(best.get(nm, 0.0), ps.value)
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clocks.get("sm_mhz") or 1965.0
+    out = {"peaks": {nm: {"value": best[nm], "unit": u, "per_sm_per_clock": best[nm] / (sms * mhz * 1e6)}
+                     for nm, u in zip(names, units)}, "sms": sms, "clocks": clocks}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,6 +511,9 @@ def main():
                     help="apply the refined and the FP64 operator once each to k columns and exit "
                          "(small case for ncu captures)")
     ap.add_argument("--columns", type=int, default=0, help="--profile-matvec: columns (default: the workload's k)")
+    ap.add_argument("--peaks", action="store_true",
+                    help="measure the arithmetic ceilings of the direct sums (FP32 FMA, packed FP32 FMA, "
+                         "MUFU rsqrt, FP64 FMA, FP64 tensor-core MMA) on this device and exit")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -507,6 +536,8 @@ def main():
     from dielectricbie_jl_b200 import _abi  # noqa: E402
     import ctypes as C
     L = _abi.lib()
+    if args.peaks:
+        return run_peaks(L, device)
     if args.workload == "cfg4":
         return run_serving_workload(args, wl, bie, device)
     if args.workload == "cfg5":

@@ -28,7 +28,7 @@ EXPORTS = [
     "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve",
     "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
     "bie_server_opts_default", "bie_server_create", "bie_server_submit", "bie_server_poll",
-    "bie_server_counters_read", "bie_server_destroy", "bie_tuning_read",
+    "bie_server_counters_read", "bie_server_destroy", "bie_tuning_read", "bie_peak_probe",
 ]
 
 
@@ -141,6 +141,7 @@ def lib():
         "bie_server_destroy": (None, [_vp]),
         "bie_tuning_read": (i, [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_double)]),
+        "bie_peak_probe": (i, [C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

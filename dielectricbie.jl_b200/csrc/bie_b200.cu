@@ -371,6 +371,18 @@ int bie_tuning_read(bie_geom* g, int32_t family, int32_t columns, int32_t pieces
     });
 }
 
+int bie_peak_probe(int32_t device, int32_t which, double* per_second, double* ms) {
+    return guarded([&] {
+        REQUIRE(per_second && ms, "peak_probe: bad argument");
+        int nd = 0;
+        if (cudaGetDeviceCount(&nd) != cudaSuccess || device < 0 || device >= nd) {
+            cudaGetLastError();
+            throw Error(BIE_EINVAL, "peak_probe: no such device");
+        }
+        bie::peak_probe(device, which, per_second, ms);
+    });
+}
+
 void bie_server_opts_default(bie_server_opts* o) {
     if (!o) return;
     o->max_slots = 4;

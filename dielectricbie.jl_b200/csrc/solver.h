@@ -43,6 +43,8 @@ void* geom_stream(bie_geom* g);
 void profile_enable(bie_geom* g, int on);
 void profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, int* ctas, double* ms);
+// Arithmetic-throughput probe `which` on `device` (peaks.cu).
+void peak_probe(int device, int which, double* per_second, double* ms);
 
 void matvec_host(bie_geom* g, const double* X, double* Y, int k, int precision, uint32_t flags);
 void matvec_device(bie_geom* g, const double* dX, double* dY, int k, int precision, uint32_t flags, cudaStream_t s);

@@ -270,6 +270,14 @@ int bie_profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 int bie_tuning_read(bie_geom* g, int32_t family, int32_t columns, int32_t pieces, int32_t* nsplit,
                     int32_t* ctas_per_sm, double* ms);
 
+/* Arithmetic-throughput probes of a device, the compute ceilings of the direct sums:
+ * which = 0 FP32 FMA, 1 FP32 FMA issued as packed f32x2 pairs, 2 MUFU reciprocal
+ * square root (FP32), 3 FP64 FMA, 4 FP64 tensor-core MMA (mma.sync m8n8k4).
+ * *per_second = lane operations per second for 0-3 (a packed f32x2 FMA counts as two)
+ * and flops per second for 4; *ms = duration of the timed launch (about 10 ms).
+ * No counterpart in the reference. */
+int bie_peak_probe(int32_t device, int32_t which, double* per_second, double* ms);
+
 /* ---- request server: the serving loop around the block solve -------------------
  * Requests of solve_dielectric_box3d_block (src/solver/multi_rhs.jl:270-286) --
  * a geometry handle, an N x k block of right-hand sides and solver options -- are
