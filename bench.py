@@ -477,8 +477,8 @@ def run_peaks(L, device):
     median sampled clock."""
     import ctypes as C
     import torch
-    names = ["fp32_fma", "fp32x2_fma", "mufu_rsqrt", "fp64_fma", "fp64_mma_m8n8k4"]
-    units = ["lane-FMA/s", "lane-FMA/s", "lane-op/s", "lane-FMA/s", "flop/s"]
+    names = ["fp32_fma", "fp32x2_fma", "mufu_rsqrt", "fp64_fma", "fp64_mma_m8n8k4", "cvt_f32x2_bf16x2"]
+    units = ["lane-FMA/s", "lane-FMA/s", "lane-op/s", "lane-FMA/s", "flop/s", "lane-op/s"]
     best = {}
     with ClockSampler(device) as clk:
         for _ in range(3):
@@ -491,8 +491,15 @@ def run_peaks(L, device):
     clocks = clk.summary()
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     mhz = clocks.get("sm_mhz") or 1965.0
+    lat = {}
+    for w, nm in ((6, "fp64_mma_m8n8k4"), (7, "fp64_fma")):
+        ps, ms = C.c_double(), C.c_double()
+        if L.bie_peak_probe(device, w, C.byref(ps), C.byref(ms)) != 0:
+            raise RuntimeError(f"bie_peak_probe({w}) failed")
+        lat[nm] = ps.value
     out = {"peaks": {nm: {"value": best[nm], "unit": u, "per_sm_per_clock": best[nm] / (sms * mhz * 1e6)}
-                     for nm, u in zip(names, units)}, "sms": sms, "clocks": clocks}
+                     for nm, u in zip(names, units)},
+           "latency_cycles": lat, "sms": sms, "clocks": clocks}
     print(json.dumps(out), flush=True)
     return 0
 
@@ -513,7 +520,8 @@ def main():
     ap.add_argument("--columns", type=int, default=0, help="--profile-matvec: columns (default: the workload's k)")
     ap.add_argument("--peaks", action="store_true",
                     help="measure the arithmetic ceilings of the direct sums (FP32 FMA, packed FP32 FMA, "
-                         "MUFU rsqrt, FP64 FMA, FP64 tensor-core MMA) on this device and exit")
+                         "MUFU rsqrt, FP64 FMA, FP64 tensor-core MMA, FP32 -> bf16x2 conversion) on this "
+                         "device and exit")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libbie_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["bie_b200.cu", "solver.cu", "blocktc.cu", "dt64mma.cu", "noalloc.cu", "server.cu", "near_gpu.cu", "peaks.cu"]
+CU_SOURCES = ["bie_b200.cu", "solver.cu", "blocktc.cu", "dt64mma.cu", "noalloc.cu", "server.cu", "near_gpu.cu", "peaks.cu", "combine_bulk.cu"]
 CPP_SOURCES = ["host_setup.cpp"]
 
 

@@ -1,6 +1,6 @@
 // Arithmetic-throughput probes: the compute ceilings of the direct sums measured
 // on the device itself (FP32 FMA scalar and packed, MUFU reciprocal square root,
-// FP64 FMA, FP64 tensor-core MMA). Every thread runs kChains independent dependency
+// FP64 FMA, FP64 tensor-core MMA, FP32 -> bf16x2 conversion). Every thread runs kChains independent dependency
 // chains of one operation for `iters` steps over a grid of several CTAs per SM, so
 // the issue and pipe rates, not latencies, set the time. The results are written
 // to a scratch buffer so the compiler keeps every chain.
@@ -91,10 +91,47 @@ __global__ void __launch_bounds__(kThreads) k_probe_dmma(float* out, int iters, 
     out[blockIdx.x * blockDim.x + threadIdx.x] = (float)s;
 }
 
+// FP32 pair -> packed bf16x2 conversion (round to nearest), the split step of the
+// tensor-core direct sum; the rounded pair is fed back as the next input.
+__global__ void __launch_bounds__(kThreads) k_probe_cvt_bf16x2(float* out, int iters, float a, float) {
+    uint32_t w[kChains];
+    float x[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) x[c] = a + threadIdx.x * 1e-3f + c;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) {
+            asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w[c]) : "f"(x[c]), "f"(x[c]));
+            x[c] = __uint_as_float(w[c]);  // the packed word read as FP32: a dependent input
+        }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) s += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Latency of dependent operations: one warp runs a single chain of `iters` FP64 MMAs
+// (lat_op 0) or FP64 FMAs (lat_op 1) and records the SM cycles it took.
+__global__ void k_probe_latency(long long* cycles, int iters, int lat_op, double a, double b) {
+    double d0 = 0.0, d1 = 0.0, x = threadIdx.x * 1e-3;
+    const long long t0 = clock64();
+    if (lat_op == 0) {
+        for (int it = 0; it < iters; ++it)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                         : "+d"(d0), "+d"(d1)
+                         : "d"(a), "d"(b));
+    } else {
+        for (int it = 0; it < iters; ++it) x = fma(x, a, b);
+    }
+    const long long t1 = clock64();
+    if (threadIdx.x == 0) cycles[0] = t1 - t0;
+    if (d0 + d1 + x == -1.0) cycles[1] = 1;  // keeps the chains
+}
+
 }  // namespace
 
 void peak_probe(int device, int which, double* per_second, double* ms_out) {
-    if (which < 0 || which > 4) throw Error(BIE_EINVAL, "peak_probe: which must be 0 .. 4");
+    if (which < 0 || which > 7) throw Error(BIE_EINVAL, "peak_probe: which must be 0 .. 7");
     int prev = 0;
     BIE_CK(cudaGetDevice(&prev));
     BIE_CK(cudaSetDevice(device));
@@ -114,13 +151,29 @@ void peak_probe(int device, int which, double* per_second, double* ms_out) {
         BIE_CK(cudaEventCreate(&e0));
         BIE_CK(cudaEventCreate(&e1));
         // steps per thread: about 10 ms per probe at the expected rates
-        const int iters = which == 4 ? 2048 : (which == 3 ? 8192 : (which == 2 ? 16384 : 65536));
+        const int iters = which == 4 ? 2048 : (which == 3 ? 8192 : (which == 2 || which == 5 ? 16384 : 65536));
+        if (which >= 6) {
+            // dependent-chain latency in SM cycles per operation (one warp)
+            const int n = 4096;
+            long long* cyc = reinterpret_cast<long long*>(out);
+            k_probe_latency<<<1, 32>>>(cyc, n, which - 6, 0.999, 1e-3);
+            BIE_CK(cudaGetLastError());
+            k_probe_latency<<<1, 32>>>(cyc, n, which - 6, 0.999, 1e-3);
+            BIE_CK(cudaGetLastError());
+            long long c = 0;
+            BIE_CK(cudaMemcpy(&c, cyc, sizeof(c), cudaMemcpyDeviceToHost));
+            *per_second = (double)c / n;
+            *ms_out = 0.0;
+            cleanup();
+            return;
+        }
         auto launch = [&] {
             switch (which) {
                 case 0: k_probe_ffma<<<ctas, kThreads>>>(out, iters, 0.999f, 1e-3f); break;
                 case 1: k_probe_ffma2<<<ctas, kThreads>>>(out, iters, 0.999f, 1e-3f); break;
                 case 2: k_probe_mufu<<<ctas, kThreads>>>(out, iters, 1.5f, 0.f); break;
                 case 3: k_probe_dfma<<<ctas, kThreads>>>(out, iters, 0.999f, 1e-3f); break;
+                case 5: k_probe_cvt_bf16x2<<<ctas, kThreads>>>(out, iters, 1.5f, 0.f); break;
                 default: k_probe_dmma<<<ctas, kThreads>>>(out, iters, 0.999f, 1e-3f); break;
             }
             BIE_CK(cudaGetLastError());

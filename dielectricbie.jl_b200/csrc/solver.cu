@@ -447,6 +447,15 @@ void combine(bie_geom* g, const TP* part, int nsplit, const double* X, double* Y
         // the block products on the FP64 tensor path, two pipeline stages
         const int nst = 2;
         const size_t sm = combine_smem_bytes(g->nb, std::min(k, kCombTile), nst);
+        // narrow blocks of right-hand sides on meshes with enough block rows to fill the
+        // GPU: the HBM-bound streaming form, where its layout conditions hold
+        // (BIE_COMBINE_ROWS forces the block-row form, for comparisons)
+        if (vl && g->npanels >= 4 * g->sms && !std::getenv("BIE_COMBINE_ROWS") &&
+            launch_combine_bulk<TP>(g->n, k, g->nb, g->npanels, part, nsplit, X, pre, dgp, rp, cl, vl, Y,
+                                    g->errflag.as<int>(), g->sms, s)) {
+            BIE_CK(cudaGetLastError());
+            return;
+        }
         const int64_t ctas = (int64_t)g->npanels * ((k + kCombTile - 1) / kCombTile);
         // long block rows of few panels: split each row into groups of blocks so that
         // about 8 CTAs per SM run (summed by k_combine_groups)

@@ -43,6 +43,12 @@ void* geom_stream(bie_geom* g);
 void profile_enable(bie_geom* g, int on);
 void profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, int* ctas, double* ms);
+// K4 streaming form (combine_bulk.cu) for k <= 16; returns false (nothing launched)
+// where its layout or alignment conditions do not hold.
+template <typename TP>
+bool launch_combine_bulk(int64_t n, int k, int nb, int npanels, const TP* part, int nsplit, const double* X,
+                         const double* pre, const double* diag, const int32_t* rowptr, const int32_t* col,
+                         const double* val, double* Y, int* err, int sms, cudaStream_t s);
 // Arithmetic-throughput probe `which` on `device` (peaks.cu).
 void peak_probe(int device, int which, double* per_second, double* ms);
 
