@@ -8,7 +8,8 @@ error behaviour) on top of the C ABI of ``libbie_b200.so``:
   near field build_neighbor_list, laplace3d_DT_corrections
   operators  lhs_dielectric_box3d, lhs_dielectric_box3d_fmm3d(_corrected),
              batched_lhs_dielectric_box3d_fmm3d_corrected (GPU operators with mul!/@),
-             rhs_dielectric_box3d, laplace3d_pottrg, dielectric_diagonal_scaling
+             rhs_dielectric_box3d, laplace3d_pottrg, dielectric_diagonal_scaling,
+             laplace3d_pottrg_fmm3d_corrected_hcubature (near-accurate probe potentials)
   solvers    solve_gmres, solve_dielectric_box3d_block, gpu_solve
 
 The mesher and the correction-block setup run on the host (as in the
@@ -36,6 +37,7 @@ __all__ = [
     "lhs_dielectric_box3d_fmm3d_corrected", "batched_lhs_dielectric_box3d_fmm3d_corrected",
     "rhs_dielectric_box3d", "laplace3d_pottrg", "dielectric_diagonal_scaling", "solve_gmres",
     "solve_dielectric_box3d_block", "gpu_solve", "polarization_energy", "BieError", "NotConverged",
+    "laplace3d_pottrg_fmm3d_corrected_hcubature", "ProbePotentialOperator",
 ]
 
 SQRT_EPS = math.sqrt(np.finfo(float).eps)
@@ -494,6 +496,91 @@ def laplace3d_pottrg(interface: DielectricInterface, targets, *, device: int = 0
     """``laplace3d_pottrg`` (src/kernel/laplace3d.jl:69-82): the M x N single-layer map at targets,
     applied on the GPU (``op @ sigma``). targets: (M, 3) or 3 x M."""
     return _PotentialOperator(interface, targets, device)
+
+
+def _targets_3xM(targets) -> np.ndarray:
+    T = np.asarray(targets, dtype=np.float64)
+    if T.ndim == 2 and T.shape[0] == 3 and T.shape[1] != 3:
+        T = T.T
+    return np.ascontiguousarray(T.reshape(-1, 3))
+
+
+class ProbePotentialOperator:
+    """Near-accurate potentials at probe points, the M x N operator of
+    ``laplace3d_pottrg_fmm3d_corrected_hcubature`` (src/kernel/laplace3d_near_hcubature.jl:278-316):
+    phi = (S_refined + C) P sigma, with the panels near the probes refined, P the
+    prolongation onto the refined nodes, S_refined their smooth-quadrature potential (GPU
+    direct sum) and C the adaptive-quadrature corrections of probes near refined non-edge
+    panels. ``op @ Sigma`` applies it on the GPU; device < 0 keeps only the host set-up."""
+
+    def __init__(self, interface: DielectricInterface, targets, hcubature_atol: float, range_factor: float,
+                 device: int = 0):
+        self.T = _targets_3xM(targets)
+        self.n = interface.n
+        self.shape = (self.T.shape[0], self.n)
+        h = C.c_void_p()
+        check(lib().bie_probe_create(interface._h, dptr(self.T), self.T.shape[0], float(hcubature_atol),
+                                     float(range_factor), int(device), C.byref(h)))
+        self._h = h
+
+    def info(self) -> dict:
+        v = [C.c_int64(), C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()]
+        check(lib().bie_probe_info(self._h, *[C.byref(x) for x in v]))
+        keys = ["n_refined", "npanels_refined", "nnz_prolongation", "nnz_corrections", "ncubatures", "capped"]
+        return {k: x.value for k, x in zip(keys, v)}
+
+    def refinement(self) -> dict:
+        """The host operator: parent coarse panel and split flag per refined panel, refined
+        corners (R, 4, 3), nodes (n_ref, 3) and weights, and P (n_ref x N) and C (M x n_ref)
+        as CSR triples (rowptr, col, val)."""
+        inf = self.info()
+        R, nr, nnp, nnc = inf["npanels_refined"], inf["n_refined"], inf["nnz_prolongation"], inf["nnz_corrections"]
+        M = self.T.shape[0]
+        out = {"parent": np.zeros(R, dtype=np.int32), "from_split": np.zeros(R, dtype=np.int32),
+               "corners": np.zeros((max(R, 1), 4, 3)), "points": np.zeros((max(nr, 1), 3)),
+               "weights": np.zeros(max(nr, 1)), "prow": np.zeros(nr + 1, dtype=np.int64),
+               "pcol": np.zeros(max(nnp, 1), dtype=np.int32), "pval": np.zeros(max(nnp, 1)),
+               "crow": np.zeros(M + 1, dtype=np.int64), "ccol": np.zeros(max(nnc, 1), dtype=np.int32),
+               "cval": np.zeros(max(nnc, 1))}
+        i64 = C.POINTER(C.c_int64)
+        check(lib().bie_probe_copy(self._h, i32ptr(out["parent"]), i32ptr(out["from_split"]), dptr(out["corners"]),
+                                   dptr(out["points"]), dptr(out["weights"]), out["prow"].ctypes.data_as(i64),
+                                   i32ptr(out["pcol"]), dptr(out["pval"]), out["crow"].ctypes.data_as(i64),
+                                   i32ptr(out["ccol"]), dptr(out["cval"])))
+        out["from_split"] = out["from_split"].astype(bool)
+        out["corners"], out["points"], out["weights"] = out["corners"][:R], out["points"][:nr], out["weights"][:nr]
+        out["pcol"], out["pval"], out["ccol"], out["cval"] = (out["pcol"][:nnp], out["pval"][:nnp],
+                                                              out["ccol"][:nnc], out["cval"][:nnc])
+        return out
+
+    def __matmul__(self, S):
+        Sf, vec = _as_cols(S, self.n)
+        k = Sf.shape[1]
+        M = self.T.shape[0]
+        phi = np.zeros((M, k), order="F")
+        check(lib().bie_probe_apply(self._h, dptr(Sf), k, dptr(phi)))
+        return phi[:, 0] if vec else phi
+
+    __mul__ = __matmul__
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().bie_probe_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def laplace3d_pottrg_fmm3d_corrected_hcubature(interface: DielectricInterface, targets, fmm_tol: float,
+                                               hcubature_atol: float, range_factor: float = 5.0, *,
+                                               device: int = 0) -> ProbePotentialOperator:
+    """``laplace3d_pottrg_fmm3d_corrected_hcubature(interface, targets, fmm_tol, hcubature_atol,
+    range_factor)`` (src/kernel/laplace3d_near_hcubature.jl:278-316). The far part is the exact
+    direct sum, so fmm_tol (the FMM's tolerance in the reference) has nothing to set."""
+    del fmm_tol
+    return ProbePotentialOperator(interface, targets, hcubature_atol, range_factor, device)
 
 
 def polarization_energy(interface: DielectricInterface, Sigma, sources, *, device: int = 0):

@@ -29,6 +29,7 @@ EXPORTS = [
     "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
     "bie_server_opts_default", "bie_server_create", "bie_server_submit", "bie_server_poll",
     "bie_server_counters_read", "bie_server_destroy", "bie_tuning_read", "bie_peak_probe",
+    "bie_probe_create", "bie_probe_info", "bie_probe_copy", "bie_probe_apply", "bie_probe_destroy",
 ]
 
 
@@ -126,6 +127,14 @@ def lib():
         "bie_potential": (i, [_vp, _dp, C.c_int32, _dp, i64, _dp]),
         "bie_potential_device": (i, [_vp, _vp, C.c_int32, _vp, i64, _vp, _vp]),
         "bie_energy": (i, [_vp, _dp, C.c_int32, _dp, _dp, _dp]),
+        "bie_probe_create": (i, [_vp, _dp, C.c_int64, C.c_double, C.c_double, C.c_int32, C.POINTER(_vp)]),
+        "bie_probe_info": (i, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                               C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "bie_probe_copy": (i, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _dp, _dp, _dp,
+                               C.POINTER(C.c_int64), C.POINTER(C.c_int32), _dp,
+                               C.POINTER(C.c_int64), C.POINTER(C.c_int32), _dp]),
+        "bie_probe_apply": (i, [_vp, _dp, C.c_int32, _dp]),
+        "bie_probe_destroy": (None, [_vp]),
         "bie_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
         "bie_solve": (i, [_vp, _dp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats)]),
         "bie_solve_device": (i, [_vp, _vp, _vp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats), _vp]),

@@ -19,8 +19,8 @@ LIB = os.path.join(HERE, "libbie_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["bie_b200.cu", "solver.cu", "blocktc.cu", "dt64mma.cu", "noalloc.cu", "server.cu", "near_gpu.cu", "peaks.cu", "combine_bulk.cu"]
-CPP_SOURCES = ["host_setup.cpp"]
+CU_SOURCES = ["bie_b200.cu", "solver.cu", "blocktc.cu", "dt64mma.cu", "noalloc.cu", "server.cu", "near_gpu.cu", "peaks.cu", "combine_bulk.cu", "probe.cu"]
+CPP_SOURCES = ["host_setup.cpp", "probe_setup.cpp"]
 
 
 def _nvcc() -> str:

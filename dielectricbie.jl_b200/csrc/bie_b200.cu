@@ -123,6 +123,11 @@ struct bie_mesh {
 struct bie_near {
     bie::Near n;
 };
+struct bie_probe {
+    bie::ProbeSetup ps;
+    bie::ProbeDev* dev = nullptr;
+    int64_t M = 0, N = 0;
+};
 
 extern "C" {
 
@@ -467,6 +472,75 @@ int bie_potential_device(bie_geom* g, const double* d_sigma, int32_t k, const do
         REQUIRE(g && d_sigma && d_targets && d_phi && k >= 1 && M >= 0, "potential_device: bad argument");
         bie::potential_device(g, d_sigma, k, d_targets, M, d_phi, (cudaStream_t)stream);
     });
+}
+
+int bie_probe_create(const bie_mesh* mh, const double* targets, int64_t M, double hcubature_atol,
+                     double range_factor, int32_t device, bie_probe** out) {
+    return guarded([&] {
+        REQUIRE(mh && out && M >= 0 && (M == 0 || targets), "probe_create: bad argument");
+        std::unique_ptr<bie_probe> p(new bie_probe());
+        std::string err;
+        if (bie::probe_setup(mh->m, targets, M, hcubature_atol, range_factor, 0, (int64_t)1 << 24, p->ps, err) != 0)
+            throw Error(BIE_EINVAL, err);
+        p->M = M;
+        p->N = mh->m.npoints();
+        if (device >= 0) {
+            int nd = 0;
+            if (cudaGetDeviceCount(&nd) != cudaSuccess || device >= nd) {
+                cudaGetLastError();
+                throw Error(BIE_ENODEVICE, "probe_create: no such CUDA device (libbie_b200 has no CPU fallback)");
+            }
+            p->dev = bie::probe_upload(p->ps, targets, M, p->N, device);
+        }
+        *out = p.release();
+    });
+}
+
+int bie_probe_info(const bie_probe* p, int64_t* n_refined, int32_t* npanels_refined, int64_t* nnz_prolongation,
+                   int64_t* nnz_corrections, int64_t* ncubatures, int64_t* capped) {
+    return guarded([&] {
+        REQUIRE(p, "probe_info: null handle");
+        if (n_refined) *n_refined = p->ps.refined.npoints();
+        if (npanels_refined) *npanels_refined = p->ps.refined.npanels;
+        if (nnz_prolongation) *nnz_prolongation = (int64_t)p->ps.pcol.size();
+        if (nnz_corrections) *nnz_corrections = (int64_t)p->ps.ccol.size();
+        if (ncubatures) *ncubatures = p->ps.ncubatures;
+        if (capped) *capped = p->ps.capped;
+    });
+}
+
+int bie_probe_copy(const bie_probe* p, int32_t* parent, int32_t* from_split, double* refined_corners,
+                   double* refined_pts, double* refined_w, int64_t* prow, int32_t* pcol, double* pval,
+                   int64_t* crow, int32_t* ccol, double* cval) {
+    return guarded([&] {
+        REQUIRE(p, "probe_copy: null handle");
+        const bie::ProbeSetup& s = p->ps;
+        if (parent) std::copy(s.parent.begin(), s.parent.end(), parent);
+        if (from_split) std::copy(s.from_split.begin(), s.from_split.end(), from_split);
+        if (refined_corners) std::copy(s.refined.corners.begin(), s.refined.corners.end(), refined_corners);
+        if (refined_pts) std::copy(s.refined.pts.begin(), s.refined.pts.end(), refined_pts);
+        if (refined_w) std::copy(s.refined.w.begin(), s.refined.w.end(), refined_w);
+        if (prow) std::copy(s.prow.begin(), s.prow.end(), prow);
+        if (pcol) std::copy(s.pcol.begin(), s.pcol.end(), pcol);
+        if (pval) std::copy(s.pval.begin(), s.pval.end(), pval);
+        if (crow) std::copy(s.crow.begin(), s.crow.end(), crow);
+        if (ccol) std::copy(s.ccol.begin(), s.ccol.end(), ccol);
+        if (cval) std::copy(s.cval.begin(), s.cval.end(), cval);
+    });
+}
+
+int bie_probe_apply(bie_probe* p, const double* Sigma, int32_t k, double* phi) {
+    return guarded([&] {
+        REQUIRE(p && Sigma && phi && k >= 1, "probe_apply: bad argument");
+        REQUIRE(p->dev, "probe_apply: the probe operator was built without a device");
+        bie::probe_apply(p->dev, Sigma, k, phi);
+    });
+}
+
+void bie_probe_destroy(bie_probe* p) {
+    if (!p) return;
+    bie::probe_free(p->dev);
+    delete p;
 }
 
 int bie_energy(bie_geom* g, const double* Sigma, int32_t k, const double* src, const double* q, double* W) {

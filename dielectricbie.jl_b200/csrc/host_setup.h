@@ -78,5 +78,24 @@ struct Near {
 // build_neighbor_list (src/kernel/laplace3d_near.jl:240-392) + laplace3d_DT_corrections
 // (src/kernel/laplace3d_near_upsampling.jl:127-276).
 int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err);
+// Near-accurate probe potentials (laplace3d_pottrg_fmm3d_corrected_hcubature,
+// src/kernel/laplace3d_near_hcubature.jl:278-316): phi = (S_refined + C) P sigma.
+struct ProbeSetup {
+    Mesh refined;                          // interface refined near the probes
+    std::vector<int> parent, from_split;   // per refined panel: coarse panel, split or not
+    std::vector<int64_t> prow;             // P: refined nodes x coarse nodes, CSR
+    std::vector<int32_t> pcol;
+    std::vector<double> pval;
+    std::vector<int64_t> crow;             // C: probes x refined nodes, CSR
+    std::vector<int32_t> ccol;
+    std::vector<double> cval;
+    int64_t nentries = 0;                  // (refined panel, near probes) entries
+    int64_t ncubatures = 0;                // adaptive integrals evaluated
+    int64_t capped = 0;                    // of which stopped at maxevals before reaching atol
+};
+// targets: 3 x M (column-major, as the reference's targets matrix); maxevals bounds each
+// adaptive integral's integrand evaluations. Returns 0, or -1 with err set.
+int probe_setup(const Mesh& m, const double* targets, int64_t M, double atol, double range_factor, int nthreads,
+                int64_t maxevals, ProbeSetup& out, std::string& err);
 
 }  // namespace bie

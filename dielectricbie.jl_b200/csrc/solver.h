@@ -49,6 +49,13 @@ template <typename TP>
 bool launch_combine_bulk(int64_t n, int k, int nb, int npanels, const TP* part, int nsplit, const double* X,
                          const double* pre, const double* diag, const int32_t* rowptr, const int32_t* col,
                          const double* val, double* Y, int* err, int sms, cudaStream_t s);
+// Near-accurate probe potentials on a device (probe.cu).
+struct ProbeSetup;
+struct ProbeDev;
+ProbeDev* probe_upload(const ProbeSetup& ps, const double* targets, int64_t M, int64_t ncoarse, int device);
+// Sigma: N x k column-major (host); phi: M x k column-major (host)
+void probe_apply(ProbeDev* d, const double* Sigma, int k, double* phi);
+void probe_free(ProbeDev* d);
 // Arithmetic-throughput probe `which` on `device` (peaks.cu).
 void peak_probe(int device, int which, double* per_second, double* ms);
 

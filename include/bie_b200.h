@@ -189,6 +189,30 @@ int bie_potential(bie_geom* g, const double* Sigma, int32_t k, const double* tar
 /* Same with device arrays: d_sigma node-major N x k, d_targets 3 x M, d_phi M x k row-major. */
 int bie_potential_device(bie_geom* g, const double* d_sigma, int32_t k, const double* d_targets, int64_t M,
                          double* d_phi, void* stream);
+/* Near-accurate probe potentials: the operator of laplace3d_pottrg_fmm3d_corrected_hcubature
+ * (src/kernel/laplace3d_near_hcubature.jl:278-316), phi = (S_refined + C) P Sigma. Panels of
+ * the mesh near the probes are split 4-way down to the smallest panel size, P interpolates
+ * Sigma onto the refined nodes, S_refined is their smooth-quadrature potential (GPU direct
+ * sum) and C corrects every probe within range_factor * l_panel / n_quad of a refined
+ * non-edge panel by that panel's adaptive integral (Genz-Malik cubature to hcubature_atol)
+ * minus its smooth-quadrature terms. targets 3 x M. device < 0 builds the host operator only
+ * (bie_probe_info / bie_probe_copy work, bie_probe_apply returns BIE_EINVAL). */
+typedef struct bie_probe bie_probe;
+int bie_probe_create(const bie_mesh* m, const double* targets, int64_t M, double hcubature_atol,
+                     double range_factor, int32_t device, bie_probe** out);
+/* Sizes: refined nodes and panels, nonzeros of P and C, adaptive integrals evaluated and
+ * how many of them stopped at the evaluation cap (2^24 per integral) before reaching atol. */
+int bie_probe_info(const bie_probe* p, int64_t* n_refined, int32_t* npanels_refined, int64_t* nnz_prolongation,
+                   int64_t* nnz_corrections, int64_t* ncubatures, int64_t* capped);
+/* Copies (any pointer may be null): parent coarse panel and split flag per refined panel,
+ * refined panel corners (npanels_refined x 4 x 3), refined nodes 3 x n_refined and weights,
+ * P in CSR (prow n_refined + 1, pcol / pval nnz) and C in CSR (crow M + 1, ccol / cval nnz). */
+int bie_probe_copy(const bie_probe* p, int32_t* parent, int32_t* from_split, double* refined_corners,
+                   double* refined_pts, double* refined_w, int64_t* prow, int32_t* pcol, double* pval,
+                   int64_t* crow, int32_t* ccol, double* cval);
+/* phi (M x k, column-major) = operator applied to Sigma (N x k, column-major). */
+int bie_probe_apply(bie_probe* p, const double* Sigma, int32_t k, double* phi);
+void bie_probe_destroy(bie_probe* p);
 /* Polarisation energy of point sources: W[c] = 1/2 q[c] S[Sigma[:, c]](src[:, c]). src 3 x k. */
 int bie_energy(bie_geom* g, const double* Sigma, int32_t k, const double* src, const double* q, double* W);
 
