@@ -91,6 +91,39 @@ __global__ void __launch_bounds__(kThreads) k_probe_dmma(float* out, int iters, 
     out[blockIdx.x * blockDim.x + threadIdx.x] = (float)s;
 }
 
+// FP64 MMA and FP64 FMA at once: even warps run the MMA chains of k_probe_dmma, odd
+// warps the FMA chains of k_probe_dfma (iters_fma steps), to see whether the two share
+// throughput.
+__global__ void __launch_bounds__(kThreads) k_probe_dmma_dfma(float* out, int iters, int iters_fma, float a,
+                                                              float b) {
+    double s = 0.0;
+    if (((threadIdx.x >> 5) & 1) == 0) {
+        double d[kChains][2];
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) d[c][0] = d[c][1] = 0.0;
+        const double av = a * (1.0 + threadIdx.x * 1e-6), bv = b;
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int c = 0; c < kChains; ++c)
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                             : "+d"(d[c][0]), "+d"(d[c][1])
+                             : "d"(av), "d"(bv));
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) s += d[c][0] + d[c][1];
+    } else {
+        double x[kChains];
+        const double ad = a, bd = b;
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) x[c] = threadIdx.x * 1e-3 + c;
+        for (int it = 0; it < iters_fma; ++it)
+#pragma unroll
+            for (int c = 0; c < kChains; ++c) x[c] = fma(x[c], ad, bd);
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) s += x[c];
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = (float)s;
+}
+
 // FP32 pair -> packed bf16x2 conversion (round to nearest), the split step of the
 // tensor-core direct sum; the rounded pair is fed back as the next input.
 __global__ void __launch_bounds__(kThreads) k_probe_cvt_bf16x2(float* out, int iters, float a, float) {
@@ -131,7 +164,7 @@ __global__ void k_probe_latency(long long* cycles, int iters, int lat_op, double
 }  // namespace
 
 void peak_probe(int device, int which, double* per_second, double* ms_out) {
-    if (which < 0 || which > 7) throw Error(BIE_EINVAL, "peak_probe: which must be 0 .. 7");
+    if (which < 0 || which > 8) throw Error(BIE_EINVAL, "peak_probe: which must be 0 .. 8");
     int prev = 0;
     BIE_CK(cudaGetDevice(&prev));
     BIE_CK(cudaSetDevice(device));
@@ -152,6 +185,28 @@ void peak_probe(int device, int which, double* per_second, double* ms_out) {
         BIE_CK(cudaEventCreate(&e1));
         // steps per thread: about 10 ms per probe at the expected rates
         const int iters = which == 4 ? 2048 : (which == 3 ? 8192 : (which == 2 || which == 5 ? 16384 : 65536));
+        if (which == 8) {
+            // half the warps on each: the same per-warp work as probes 4 and 3, so with
+            // separate pipes the launch takes about as long as the slower half alone
+            const int it4 = 2048 / 2, it3 = 8192 / 2;
+            auto mixed = [&] {
+                k_probe_dmma_dfma<<<ctas, kThreads>>>(out, it4, it3, 0.999f, 1e-3f);
+                BIE_CK(cudaGetLastError());
+            };
+            mixed();
+            BIE_CK(cudaEventRecord(e0));
+            mixed();
+            BIE_CK(cudaEventRecord(e1));
+            BIE_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BIE_CK(cudaEventElapsedTime(&ms, e0, e1));
+            const double half = (double)ctas * kThreads / 2.0;
+            // reported: MMA flop/s of the even warps (the FMA lane rate follows from ms)
+            *per_second = half / 32.0 * kChains * (double)it4 * 512.0 / (ms * 1e-3);
+            *ms_out = ms;
+            cleanup();
+            return;
+        }
         if (which >= 6) {
             // dependent-chain latency in SM cycles per operation (one warp)
             const int n = 4096;

@@ -298,7 +298,9 @@ int bie_tuning_read(bie_geom* g, int32_t family, int32_t columns, int32_t pieces
  * which = 0 FP32 FMA, 1 FP32 FMA issued as packed f32x2 pairs, 2 MUFU reciprocal
  * square root (FP32), 3 FP64 FMA, 4 FP64 tensor-core MMA (mma.sync m8n8k4), 5 FP32 pair to
  * packed bf16x2 conversion (cvt.rn.bf16x2.f32); 6 and 7: latency of a dependent chain of
- * FP64 tensor-core MMAs (6) or FP64 FMAs (7), one warp.
+ * FP64 tensor-core MMAs (6) or FP64 FMAs (7), one warp; 8: FP64 MMAs and FP64 FMAs at once
+ * (half the warps each, a quarter of probes 4 and 3's work each; *per_second = the MMA
+ * flop rate, *ms = the launch), to show whether the two share throughput.
  * *per_second = lane operations per second for 0-3 and 5 (a packed f32x2 FMA counts as two),
  * flops per second for 4, and SM cycles per operation for 6 and 7 (the "per second" name
  * notwithstanding); *ms = duration of the timed launch (about 10 ms; 0 for 6 and 7).
