@@ -679,7 +679,7 @@ __global__ void k_axpby(double a, const double* __restrict__ X, double b, double
 // Givens step of iteration j for every active column (one thread per column).
 // R: [(m+1) x (m+1) x k] column j holds h[0..j+1]; cs/sn: [m x k]; gv: [(m+1) x k].
 __global__ void k_givens(double* __restrict__ R, const double* __restrict__ h /*[(j+1) x k]*/,
-                         const double* __restrict__ h2 /*[(j+1) x k], second Gram-Schmidt pass*/,
+                         const double* __restrict__ h2 /*[(j+1) x k], second Gram-Schmidt pass, or null*/,
                          const double* __restrict__ hnorm /*[k]*/, double* __restrict__ cs, double* __restrict__ sn,
                          double* __restrict__ gv, int* __restrict__ active, int* __restrict__ jlast,
                          const double* __restrict__ eps, double* __restrict__ resid, int j, int m1, int k) {
@@ -687,7 +687,7 @@ __global__ void k_givens(double* __restrict__ R, const double* __restrict__ h /*
     if (c >= k) return;
     if (!active[c]) return;
     double* Rj = R + ((int64_t)j * m1) * k;  // column j: Rj[i * k + c]
-    for (int i = 0; i <= j; ++i) Rj[i * k + c] = h[i * k + c] + h2[i * k + c];
+    for (int i = 0; i <= j; ++i) Rj[i * k + c] = h[i * k + c] + (h2 ? h2[i * k + c] : 0.0);
     Rj[(j + 1) * k + c] = hnorm[c];
     for (int i = 0; i < j; ++i) {
         double a = Rj[i * k + c], b = Rj[(i + 1) * k + c];

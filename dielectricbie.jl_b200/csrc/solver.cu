@@ -599,12 +599,17 @@ struct GmresResult {
 // Solves A(prec) (p .* u) = r, x = p .* u for the columns flagged in `active0`;
 // dx (node-major n x k) receives the solution (zeroed first). eps[c] is the
 // absolute residual tolerance of column c. Each column runs its own Arnoldi
-// process with classical Gram-Schmidt applied twice; converged columns are frozen.
+// process; converged columns are frozen. FP64 solves orthogonalise by classical
+// Gram-Schmidt applied twice. The inner solves of iterative refinement (reduced
+// precision operators) stop at a relative residual of about 1e-6, and the outer
+// loop recomputes the true residual, so one classical Gram-Schmidt pass (fused with
+// the new direction's norm) serves them and halves the passes over the basis.
 GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, int check_every,
                   cudaStream_t s) {
     const int64_t n = g->n;
     const int64_t nk = n * (int64_t)k;
+    const bool one_pass = prec != BIE_FP64;  // see above
     m = std::max(1, std::min(m, itmax));
     const int m1 = m + 1;
     g->V.ensure(sizeof(double) * (size_t)m1 * nk);
@@ -715,22 +720,28 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             auto iteration = [&]() {
                 double* Vj = V + (size_t)j * nk;
                 apply_op(g, Vj, W, k, prec, flags, pre, s);
-                // classical Gram-Schmidt, twice; the second pass is fused with the norm of the
-                // new direction and its coefficients are added to the first pass's in the Givens step
+                // classical Gram-Schmidt, twice for FP64 solves; the last pass is fused with the
+                // norm of the new direction, and the second pass's coefficients are added to the
+                // first pass's in the Givens step
                 dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
-                {
-                    Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                    k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+                if (one_pass) {
+                    gs_update_norm(g, W, V, nk, j + 1, g->h.as<double>(), k, g->hn.as<double>(), s);
+                } else {
+                    {
+                        Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                        k_gs_update<<<grid1(nk), 256, 0, s>>>(W, V, nk, j + 1, g->h.as<double>(), n, k);
+                    }
+                    dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
+                    gs_update_norm(g, W, V, nk, j + 1, g->h2.as<double>(), k, g->hn.as<double>(), s);
                 }
-                dots(g, V, nk, j + 1, W, k, g->h2.as<double>(), 0, s);
-                gs_update_norm(g, W, V, nk, j + 1, g->h2.as<double>(), k, g->hn.as<double>(), s);
                 {
                     Prof pf(g, BIE_KERNEL_KRYLOV, s);
                     k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), n, k, V + (size_t)(j + 1) * nk);
                 }
                 {
                     Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                    k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), g->h2.as<double>(),
+                    k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(),
+                                                        one_pass ? nullptr : g->h2.as<double>(),
                                                         g->hn.as<double>(), g->cs.as<double>(), g->sn.as<double>(),
                                                         g->gv.as<double>(), g->active.as<int>(), g->jlast.as<int>(),
                                                         g->eps.as<double>(), g->resid.as<double>(), j, m1, k);
