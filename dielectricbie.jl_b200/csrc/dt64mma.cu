@@ -8,8 +8,11 @@
 // Same operator as laplace3d_DT (src/kernel/laplace3d.jl:30-40) / lfmm3d pg=2
 // (src/kernel/laplace3d.jl:100-107); the 1/(4 pi) is applied by the combine.
 //
-// CTA = 4 warps = 128 targets; a warp owns 32 targets (four 8-row m-tiles) and NC
-// columns (NC/8 n-tiles). Per k-step of 4 sources each thread generates the four
+// CTA = 4 warps = 64 targets; a warp owns 16 targets (MTW = 2 8-row m-tiles) and NC
+// columns (NC/8 n-tiles). Two m-tiles per warp keep the accumulators at 2 x NC
+// doubles, so three CTAs fit per SM (measured 10 % faster at NC = 64 than four m-tiles
+// per warp at two CTAs per SM; FP64 MMA and FP64 FMA share one throughput budget, and
+// more resident warps overlap the kernel-value generation with the MMAs). Per k-step of 4 sources each thread generates the four
 // FP64 kernel values of its A fragments (target = m-tile row l/4, source = l%4)
 // and loads its B fragments (source l%4, column l/4 of each n-tile) from shared
 // memory; 4 x NC/8 DMMAs follow. Box faces are axis-aligned, so a warp whose 32
@@ -26,7 +29,9 @@
 namespace bie {
 namespace d64 {
 
-constexpr int TB = 128;   // targets per CTA
+constexpr int MTW = 2;  // m-tiles per warp
+constexpr int NTHR = 128;  // threads per CTA
+constexpr int TB = 32 * MTW;   // targets per CTA
 constexpr int TSRC = 32;  // sources per shared-memory tile
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
@@ -52,37 +57,37 @@ __device__ __forceinline__ double kernel_val(double tx, double ty, double tz, do
 template <int NC, int AX>
 __device__ __forceinline__ void tile_step(const double* __restrict__ ssx, const double* __restrict__ ssy,
                                           const double* __restrict__ ssz, const double* __restrict__ sq, int cnt,
-                                          const double (&tx)[4], const double (&ty)[4], const double (&tz)[4],
-                                          const double (&tn)[4][3], double (&acc)[4][NC / 8][2], int lane,
-                                          bool self, int64_t jt, const int64_t (&ti)[4]) {
+                                          const double (&tx)[MTW], const double (&ty)[MTW], const double (&tz)[MTW],
+                                          const double (&tn)[MTW][3], double (&acc)[MTW][NC / 8][2], int lane,
+                                          bool self, int64_t jt, const int64_t (&ti)[MTW]) {
     constexpr int LDQ = NC + 8;
     const int kq = lane & 3, grp = lane >> 2;
 #pragma unroll 2
     for (int k0 = 0; k0 < cnt; k0 += 4) {
         const int j = k0 + kq;
         const double sx = ssx[j], sy = ssy[j], sz = ssz[j];
-        double a[4];
+        double a[MTW];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
+        for (int mt = 0; mt < MTW; ++mt) {
             a[mt] = kernel_val<AX>(tx[mt], ty[mt], tz[mt], tn[mt][0], tn[mt][1], tn[mt][2], sx, sy, sz);
             if (self && jt + j == ti[mt]) a[mt] = 0.0;
         }
         if (j >= cnt) {
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt) a[mt] = 0.0;
+            for (int mt = 0; mt < MTW; ++mt) a[mt] = 0.0;
         }
         double b[NC / 8];
 #pragma unroll
         for (int nt = 0; nt < NC / 8; ++nt) b[nt] = sq[j * LDQ + nt * 8 + grp];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
+        for (int mt = 0; mt < MTW; ++mt)
 #pragma unroll
             for (int nt = 0; nt < NC / 8; ++nt) dmma(acc[mt][nt][0], acc[mt][nt][1], a[mt], b[nt]);
     }
 }
 
 template <int NC>
-__global__ void __launch_bounds__(TB, 2) k_dt_f64_mma(GeomDev g, const double* __restrict__ X, int ldx, int c0,
+__global__ void __launch_bounds__(NTHR, 3) k_dt_f64_mma(GeomDev g, const double* __restrict__ X, int ldx, int c0,
                                                      int kc, const double* __restrict__ pre, int64_t chunk,
                                                      double* __restrict__ part, int ldp) {
     constexpr int LDQ = NC + 8;  // padded row: conflict-free B-fragment loads
@@ -91,13 +96,13 @@ __global__ void __launch_bounds__(TB, 2) k_dt_f64_mma(GeomDev g, const double* _
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane >> 2, kq = lane & 3;
     const int64_t i0 = (int64_t)blockIdx.x * TB;
-    const int64_t wbase = i0 + warp * 32;
-    // the warp's 32 targets: m-tile mt, row grp -> target wbase + 8 mt + grp
-    double tx[4], ty[4], tz[4], tn[4][3];
-    int64_t ti[4];
+    const int64_t wbase = i0 + warp * 8 * MTW;
+    // the warp's 8 MTW targets: m-tile mt, row grp -> target wbase + 8 mt + grp
+    double tx[MTW], ty[MTW], tz[MTW], tn[MTW][3];
+    int64_t ti[MTW];
     int code_min = 4, code_max = -1;
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
+    for (int mt = 0; mt < MTW; ++mt) {
         const int64_t i = wbase + mt * 8 + grp;
         ti[mt] = i;
         if (i < g.n) {
@@ -118,9 +123,9 @@ __global__ void __launch_bounds__(TB, 2) k_dt_f64_mma(GeomDev g, const double* _
     code_min = __reduce_min_sync(full, code_min);
     code_max = __reduce_max_sync(full, code_max);
     const int ax = (code_min == code_max && code_min < 3) ? code_min : 3;
-    double acc[4][NC / 8][2];
+    double acc[MTW][NC / 8][2];
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
+    for (int mt = 0; mt < MTW; ++mt)
 #pragma unroll
         for (int nt = 0; nt < NC / 8; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
 
@@ -129,14 +134,14 @@ __global__ void __launch_bounds__(TB, 2) k_dt_f64_mma(GeomDev g, const double* _
     for (int64_t jt = j0; jt < j1; jt += TSRC) {
         const int cnt = (int)min((int64_t)TSRC, j1 - jt);
         __syncthreads();
-        for (int t = threadIdx.x; t < TSRC + 4; t += TB) {
+        for (int t = threadIdx.x; t < TSRC + 4; t += NTHR) {
             const int64_t j = jt + t;
             const bool v = t < cnt;
             ssx[t] = v ? g.x[j] : 1.0e150;
             ssy[t] = v ? g.y[j] : 1.0e150;
             ssz[t] = v ? g.z[j] : 1.0e150;
         }
-        for (int e = threadIdx.x; e < TSRC * NC; e += TB) {
+        for (int e = threadIdx.x; e < TSRC * NC; e += NTHR) {
             const int t = e / NC, c = e - t * NC;
             const int64_t j = jt + t;
             double q = 0.0;
@@ -154,7 +159,7 @@ __global__ void __launch_bounds__(TB, 2) k_dt_f64_mma(GeomDev g, const double* _
     }
     // D fragment: (row grp, columns 2 kq, 2 kq + 1) of each (m-tile, n-tile)
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
+    for (int mt = 0; mt < MTW; ++mt) {
         const int64_t i = ti[mt];
         if (i >= g.n) continue;
         const double sgn = ax == 0 ? tn[mt][0] : ax == 1 ? tn[mt][1] : ax == 2 ? tn[mt][2] : 1.0;
@@ -175,13 +180,13 @@ void launch_dt_f64_mma(const GeomDev& g, const double* X, int ldx, int c0, int k
                        int64_t chunk, double* part, int ldp, cudaStream_t s) {
     dim3 grid((unsigned)((g.n + d64::TB - 1) / d64::TB), (unsigned)nsplit);
     if (kc > 32)
-        d64::k_dt_f64_mma<64><<<grid, d64::TB, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
+        d64::k_dt_f64_mma<64><<<grid, d64::NTHR, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
     else if (kc > 16)
-        d64::k_dt_f64_mma<32><<<grid, d64::TB, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
+        d64::k_dt_f64_mma<32><<<grid, d64::NTHR, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
     else if (kc > 8)
-        d64::k_dt_f64_mma<16><<<grid, d64::TB, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
+        d64::k_dt_f64_mma<16><<<grid, d64::NTHR, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
     else
-        d64::k_dt_f64_mma<8><<<grid, d64::TB, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
+        d64::k_dt_f64_mma<8><<<grid, d64::NTHR, 0, s>>>(g, X, ldx, c0, kc, pre, chunk, part, ldp);
     BIE_CK(cudaGetLastError());
 }
 

@@ -295,7 +295,7 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
                  int64_t M, cudaStream_t s) {
     GeomDev gd = gdev(g);
     if (kind == Kern::DT64 && k >= 8) {
-        // FP64 tensor-core contraction, 64 columns per launch, 2 CTAs of 128 targets per SM;
+        // FP64 tensor-core contraction, 64 columns per launch, 3 CTAs of 64 targets per SM;
         // the source split count is autotuned around the occupancy model's
         const double npairs = (double)g->n * (g->n - 1);
         auto run = [&](const Split& sp, bool prof) {
@@ -307,16 +307,19 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
                 launch_dt_f64_mma(gd, X, ldx, c0, kc, pre, sp.nsplit, sp.chunk, g->part.as<double>(), k, s);
             }
         };
+        // (the split model of 128-row tiles at two CTAs per SM, which gives the 64-target
+        // CTAs about twice the source splits of a full wave: measured faster than the model
+        // matched to 64-target CTAs at three per SM)
         const Split base = choose_split(g->n, g->n, g->sms, 2);
         const auto key = std::make_tuple(1, std::min(k, 64), 0);
         auto it = g->tuned.find(key);
         if (it == g->tuned.end() && can_tune(g, s)) {
-            std::vector<bie_geom::Tuned> cands{{base.nsplit, base.chunk, 2, 0.0}};
+            std::vector<bie_geom::Tuned> cands{{base.nsplit, base.chunk, 3, 0.0}};
             for (int64_t ns : {(int64_t)base.nsplit / 2, 2 * (int64_t)base.nsplit}) {
                 const Split sp = dt64_split_n(g, ns);
                 bool dup = false;
                 for (auto& c : cands) dup = dup || c.nsplit == sp.nsplit;
-                if (!dup) cands.push_back({sp.nsplit, sp.chunk, 2, 0.0});
+                if (!dup) cands.push_back({sp.nsplit, sp.chunk, 3, 0.0});
             }
             it = g->tuned.emplace(key, tune(g, s, cands, [&](const bie_geom::Tuned& c) {
                                        run(Split{c.nsplit, c.chunk}, false);
