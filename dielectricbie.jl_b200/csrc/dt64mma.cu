@@ -60,7 +60,7 @@ __device__ __forceinline__ void tile_step(const double* __restrict__ ssx, const 
                                           const double (&tx)[MTW], const double (&ty)[MTW], const double (&tz)[MTW],
                                           const double (&tn)[MTW][3], double (&acc)[MTW][NC / 8][2], int lane,
                                           bool self, int64_t jt, const int64_t (&ti)[MTW]) {
-    constexpr int LDQ = NC + 8;
+    constexpr int LDQ = NC + 4;
     const int kq = lane & 3, grp = lane >> 2;
 #pragma unroll 2
     for (int k0 = 0; k0 < cnt; k0 += 4) {
@@ -90,7 +90,9 @@ template <int NC>
 __global__ void __launch_bounds__(NTHR, 3) k_dt_f64_mma(GeomDev g, const double* __restrict__ X, int ldx, int c0,
                                                      int kc, const double* __restrict__ pre, int64_t chunk,
                                                      double* __restrict__ part, int ldp) {
-    constexpr int LDQ = NC + 8;  // padded row: conflict-free B-fragment loads
+    // padded row of NC + 4 doubles (4 mod 16): the four k-rows a half-warp's B-fragment
+    // load touches fall on distinct banks
+    constexpr int LDQ = NC + 4;
     __shared__ double ssx[TSRC + 4], ssy[TSRC + 4], ssz[TSRC + 4];
     __shared__ double sq[(TSRC + 4) * LDQ];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
