@@ -518,6 +518,8 @@ def main():
                     help="apply the refined and the FP64 operator once each to k columns and exit "
                          "(small case for ncu captures)")
     ap.add_argument("--columns", type=int, default=0, help="--profile-matvec: columns (default: the workload's k)")
+    ap.add_argument("--cfg4-requests", type=int, default=0, help="--workload cfg4: requests (default 120)")
+    ap.add_argument("--cfg4-nmax", type=int, default=0, help="--workload cfg4: largest node count (default 30000)")
     ap.add_argument("--peaks", action="store_true",
                     help="measure the arithmetic ceilings of the direct sums (FP32 FMA, packed FP32 FMA, "
                          "MUFU rsqrt, FP64 FMA, FP64 tensor-core MMA, FP32 -> bf16x2 conversion) on this "
@@ -547,6 +549,11 @@ def main():
     if args.peaks:
         return run_peaks(L, device)
     if args.workload == "cfg4":
+        wl = dict(wl)
+        if args.cfg4_requests:
+            wl["requests"] = args.cfg4_requests
+        if args.cfg4_nmax:
+            wl["n_max"] = args.cfg4_nmax
         return run_serving_workload(args, wl, bie, device)
     if args.workload == "cfg5":
         return run_lattice_workload(args, wl, bie, device)

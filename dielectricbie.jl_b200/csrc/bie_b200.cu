@@ -584,6 +584,7 @@ int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, c
         bie_solve_opts d;
         bie_solve_opts_default(&d);
         rc = bie::solve_device(g, dF, dSigma, k, o ? *o : d, st, (cudaStream_t)stream);
+        bie::geom_trim_if_short(g);
     });
     return grc != BIE_OK ? grc : rc;
 }

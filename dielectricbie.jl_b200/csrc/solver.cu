@@ -931,6 +931,38 @@ bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, 
     return true;
 }
 
+// Releases a geometry's operator and solver workspace (direct-sum partials, Krylov
+// basis, staging buffers) and the CUDA graphs that point into it; the geometry itself
+// stays resident and the next call allocates again. solve_host and the device solve
+// entry do this after a solve when less than a quarter of the device memory is free
+// (or always, with the environment variable BIE_TRIM_WORKSPACE), so that many resident
+// geometries solved in turn (a server's) do not keep a workspace each until the device
+// runs out. The workspace is sized for the restart length: (restart + 1) N k doubles.
+void geom_trim(bie_geom* g) {
+    DeviceGuard dg(g->device);
+    BIE_CK(cudaStreamSynchronize(g->stream));
+    bie::Buf* ws[] = {&g->part, &g->bpack, &g->cpart, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn, &g->h, &g->h2,
+                      &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid, &g->dpart, &g->rr,
+                      &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
+    for (auto* b : ws) b->release();
+    for (auto& c : g->gcache) {
+        for (auto ex : c.exec)
+            if (ex) cudaGraphExecDestroy(ex);
+        c.exec.clear();
+        c.sig = 0;
+        c.warm = false;
+    }
+}
+
+void geom_trim_if_short(bie_geom* g) {
+    DeviceGuard dg(g->device);
+    size_t fr = 0, tot = 0;
+    if (std::getenv("BIE_TRIM_WORKSPACE") ||
+        (cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr < tot / 4))
+        geom_trim(g);
+    cudaGetLastError();
+}
+
 void geom_destroy(bie_geom* g) {
     {
         DeviceGuard dg(g->device);
@@ -1277,6 +1309,7 @@ int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_sol
     BIE_CK(cudaGetLastError());
     BIE_CK(cudaMemcpyAsync(Sigma, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));
+    geom_trim_if_short(g);
     return rc;
 }
 

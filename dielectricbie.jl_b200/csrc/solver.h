@@ -38,6 +38,10 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
                       int32_t npanels, int32_t nb, const int32_t* rowptr, const int32_t* col, const double* val,
                       int64_t nblocks, int device);
 void geom_destroy(bie_geom* g);
+// Releases the geometry's operator/solver workspace and graphs (see solver.cu); the
+// _if_short form does so only when less than a quarter of device memory is free.
+void geom_trim(bie_geom* g);
+void geom_trim_if_short(bie_geom* g);
 void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes);
 void* geom_stream(bie_geom* g);
 void profile_enable(bie_geom* g, int on);

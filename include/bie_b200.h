@@ -254,6 +254,11 @@ typedef struct {
  * Arnoldi process; converged columns are frozen). With precision != BIE_FP64 the
  * Krylov operator is the reduced-precision one inside FP64 iterative refinement.
  * Host arrays N x k. Returns BIE_ENOCONV (with Sigma filled) when itmax is hit. */
+/* After a solve (bie_solve, bie_solve_device) the library releases the handle's solver
+ * workspace, about (restart + 1) N k doubles, when less than a quarter of the device
+ * memory is free (always with the environment variable BIE_TRIM_WORKSPACE), so that many
+ * resident geometries solved in turn do not keep a workspace each. The next solve
+ * allocates it again. */
 int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st);
 int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o,
                      bie_stats* st, void* stream);

@@ -229,3 +229,20 @@ def test_autotuned_launch_recorded_and_accurate(bie, cfg1, rng):
     assert t_64 is not None and t_64["nsplit"] >= 1
     assert rel(Y64, A @ X + Cm @ X) < 1e-13
     assert rel(Y3, Y64) < 5e-5
+
+
+def test_workspace_trim_keeps_results(bie, cfg1, monkeypatch):
+    """Solves after the solver workspace was released (BIE_TRIM_WORKSPACE: after every
+    solve) reallocate it and recapture their graphs, and give the same sigma."""
+    itf, m, Cm, A = cfg1
+    op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, 1e-9, 8, precision="bf16x3")
+    src = [bie.PointSource((0.1, 0.1, 0.1), 1.0), bie.PointSource((-0.2, 0.05, 0.0), -0.5)] * 4
+    F = bie.rhs_dielectric_box3d(itf, src, 4.0)
+    S0, _ = bie.gpu_solve(op, F, rtol=1e-10)
+    S1, _ = bie.gpu_solve(op, F, rtol=1e-10)
+    monkeypatch.setenv("BIE_TRIM_WORKSPACE", "1")
+    S2, st2 = bie.gpu_solve(op, F, rtol=1e-10)
+    S3, st3 = bie.gpu_solve(op, F, rtol=1e-10)
+    assert st2.solved and st3.solved
+    for S in (S1, S2, S3):
+        assert rel(S, S0) < 1e-13
