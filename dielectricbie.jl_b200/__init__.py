@@ -289,14 +289,25 @@ class _Near:
         self.nblocks, self.nb, self.hit_max_depth = nbl.value, nb.value, bool(hm.value)
         self.rowptr = np.zeros(itf.npanels + 1, dtype=np.int32)
         self.col = np.zeros(self.nblocks, dtype=np.int32)
-        self.val = np.zeros(self.nblocks * self.nb * self.nb)
+        self._val = None  # the block values stay in the library's copy until asked for
         ui, uj, up = (np.zeros(nu.value, dtype=np.int32) for _ in range(3))
         ai, aj = (np.zeros(na.value, dtype=np.int32) for _ in range(2))
-        check(lib().bie_near_copy(h, i32ptr(self.rowptr), i32ptr(self.col), dptr(self.val), i32ptr(ui), i32ptr(uj),
+        check(lib().bie_near_copy(h, i32ptr(self.rowptr), i32ptr(self.col), None, i32ptr(ui), i32ptr(uj),
                                   i32ptr(up), i32ptr(ai), i32ptr(aj)))
         self.upsample = {(int(i), int(j)): int(p) for i, j, p in zip(ui, uj, up)}
         self.adaptive = {(int(i), int(j)): ad for i, j in zip(ai, aj)}
         self.n = itf.n
+
+    @property
+    def val(self) -> np.ndarray:
+        """Correction block values (nblocks x nb x nb, each block column-major), copied out
+        of the library on first use; a geometry that is only solved on the device never
+        holds a second host copy of its blocks."""
+        if self._val is None:
+            v = np.zeros(self.nblocks * self.nb * self.nb)
+            check(lib().bie_near_copy(self._h, None, None, dptr(v), None, None, None, None, None))
+            self._val = v
+        return self._val
 
     def __del__(self):
         try:
