@@ -84,3 +84,22 @@ def assemble(op, sigma):
     M = op.T.shape[0]
     return (smooth_potential(R["points"], R["weights"], s_ref, op.T)
             + csr_apply(R["crow"], R["ccol"], R["cval"], s_ref, M)), s_ref, R
+
+
+def pottrg_near(itf, sigma, t, range_factor=5.0):
+    """laplace3d_pottrg_near (src/kernel/laplace3d_near.jl:447-508): panels whose centre is
+    within range_factor * max(|b - a|, |d - a|) / n_quad of t are integrated exactly (here by
+    the quadtree Gauss rule of interp_potential), the others by their smooth quadrature."""
+    t = np.asarray(t, dtype=float)
+    nq = itf.n_quad
+    q2 = nq * nq
+    glx, bary = np.asarray(itf.panels[0].gl_xs), np.asarray(itf.panels[0].bary_weights)
+    c = itf.corners
+    cc = c.mean(axis=1)
+    l_panel = np.maximum(np.linalg.norm(c[:, 1] - c[:, 0], axis=1), np.linalg.norm(c[:, 3] - c[:, 0], axis=1))
+    near = np.linalg.norm(cc - t[None, :], axis=1) <= range_factor * l_panel / nq
+    far_nodes = np.repeat(~near, q2)
+    val = float(smooth_potential(itf.points[far_nodes], itf.weights[far_nodes], sigma[far_nodes], t[None, :])[0])
+    for p in np.where(near)[0]:
+        val += interp_potential(c[p], glx, bary, sigma[p * q2:(p + 1) * q2], t)
+    return val
