@@ -2,7 +2,8 @@
 on the library's mesher: a single box equals single_dielectric_box3d; touching boxes share
 their common face once, with (eps of the box the normal leaves, eps of the other) on it, and
 the quadrature weights integrate the exposed plus shared area; a two-box system solves with
-finite sigma. No GPU except the solve."""
+finite sigma. Also the corner-pair discovery case of build_neighbor_list. No GPU except
+the solve."""
 import numpy as np
 import pytest
 
@@ -54,3 +55,24 @@ def test_two_box_solver_integration(bie):
     assert op.shape == (itf.n, itf.n) and rhs.shape == (itf.n,)
     sigma, st = bie.gpu_solve(op, rhs, rtol=1e-10, precision="fp64")
     assert sigma.shape == (itf.n,) and np.all(np.isfinite(sigma)) and st.solved
+
+
+def test_corner_pair_discovery(bie, orc):
+    """build_neighbor_list corner-pair discovery (test/kernel/laplace3d_near_corner_pairs.jl):
+    two perpendicular n_quad = 3 panels sharing an edge, whose Gauss nodes are all interior,
+    form a touching (adaptive) pair exactly when correct_edges is set; library and oracle."""
+    ns, ws = bie.gausslegendre(3)
+    pa = bie.rect_panel3d_discretize((-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0),
+                                     ns, ws, (0.0, 0.0, 1.0))
+    pb = bie.rect_panel3d_discretize((0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (0.5, 0.5, 1.0), (0.5, -0.5, 1.0),
+                                     ns, ws, (1.0, 0.0, 0.0))
+    itf = bie.DielectricInterface([pa, pb], [1.0, 1.0], [1.0, 1.0])
+    _, adaptive = bie.build_neighbor_list(itf, 8, 1e-6, correct_edges=False)
+    assert not adaptive
+    itf2 = bie.DielectricInterface([pa, pb], [1.0, 1.0], [1.0, 1.0])
+    _, adaptive = bie.build_neighbor_list(itf2, 8, 1e-6, correct_edges=True)
+    assert (0, 1) in adaptive or (1, 0) in adaptive
+    m = orc.Mesh.from_panels(3, [itf.corners[0], itf.corners[1]], [[0, 0, 1], [1, 0, 0]])
+    assert not orc.build_neighbor_list(m, 8, 1e-6, False)[1]
+    adp = orc.build_neighbor_list(m, 8, 1e-6, True)[1]
+    assert set(map(tuple, adp)) & {(0, 1), (1, 0)}
