@@ -243,7 +243,7 @@ def poisson_arrivals(rng, count, rate):
     return np.cumsum(rng.exponential(1.0 / rate, size=count)) - 0.0
 
 
-def serve_stream(bie, requests, precision, rtol, slots=4, batch=64):
+def serve_stream(bie, requests, precision, rtol, slots=4, batch=128):
     """Serves `requests` = [(op, F, arrival_s)] through the library's request server
     (continuous batching), submitting each at its arrival time from a separate thread.
     Latency = completion - arrival; throughput = RHS columns / (last completion - first arrival)."""

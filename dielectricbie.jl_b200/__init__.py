@@ -679,7 +679,7 @@ class SolveServer:
     An operator handed to a server must not be used directly until its requests
     have been collected."""
 
-    def __init__(self, *, max_slots: int = 4, max_batch_rhs: int = 64, hbm_fraction: float = 0.8, device: int = 0):
+    def __init__(self, *, max_slots: int = 4, max_batch_rhs: int = 128, hbm_fraction: float = 0.8, device: int = 0):
         o = _abi.ServerOpts()
         lib().bie_server_opts_default(C.byref(o))
         o.max_slots, o.max_batch_rhs, o.hbm_fraction, o.device = int(max_slots), int(max_batch_rhs), \

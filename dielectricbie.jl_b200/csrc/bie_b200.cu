@@ -391,7 +391,7 @@ int bie_peak_probe(int32_t device, int32_t which, double* per_second, double* ms
 void bie_server_opts_default(bie_server_opts* o) {
     if (!o) return;
     o->max_slots = 4;
-    o->max_batch_rhs = 64;
+    o->max_batch_rhs = 128;
     o->hbm_fraction = 0.8;
     o->device = 0;
 }

@@ -325,7 +325,7 @@ typedef struct bie_server bie_server;
 
 typedef struct {
     int max_slots;       /* block solves in flight at once (default 4) */
-    int max_batch_rhs;   /* columns merged into one block solve (default 64, <= 256) */
+    int max_batch_rhs;   /* columns merged into one block solve (default 128, <= 256) */
     double hbm_fraction; /* admission budget: this fraction of the device's free memory at creation (0.8) */
     int device;          /* CUDA device of the budget (the geometries carry their own) */
 } bie_server_opts;
