@@ -657,8 +657,10 @@ def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float 
 
 def tuned_launch(op: "GPUDielectricOperator", family: str, k: int, pieces: int = 2):
     """The autotuned launch configuration the library chose for an operator's direct sum:
-    family "tensor_core" (columns = min(k, 128)) or "fp64" (columns = min(k, 64)).
-    Returns dict(nsplit, ctas_per_sm, ms) or None when nothing was tuned yet."""
+    family "tensor_core" (columns = min(k, 128)) or "fp64" (columns = min(k, 64)). Every width
+    that runs the same kernel instance (a multiple of 16 for "tensor_core"; 8, 16, 32 or 64
+    for "fp64") shares one entry. Returns dict(nsplit, ctas_per_sm, ms) or None when nothing
+    was tuned yet."""
     fam, cols, pc = (0, min(k, 128), pieces) if family == "tensor_core" else (1, min(k, 64), 0)
     ns, ct, ms = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
     rc = lib().bie_tuning_read(op.geom._h, fam, cols, pc, C.byref(ns), C.byref(ct), C.byref(ms))

@@ -53,7 +53,7 @@ struct bie_geom {
     GraphCache gcache[2];
     int gcache_next = 0;
     bool graphs = true;  // off with the environment variable BIE_NO_GRAPHS
-    // autotuned launch configurations of the direct sums, keyed by (family, columns, pieces)
+    // autotuned launch configurations of the direct sums, keyed by tune_key(family, columns, pieces)
     struct Tuned {
         int nsplit;
         int64_t chunk;
@@ -249,6 +249,16 @@ Split dt64_split_n(const bie_geom* g, int64_t ns) {
     return Split{(int)((g->n + chunk - 1) / chunk), chunk};
 }
 
+// Autotuner key of a direct-sum family at a column width: the width is rounded up to the
+// kernel instance the launch runs (K3: the MMA width, a multiple of 16, of the first block
+// of at most 128 columns; K1: the 8/16/32/64-column template of the first block of at most
+// 64), so that a server's batches of different widths share one tuning per instance.
+std::tuple<int, int, int> tune_key(int family, int columns, int pieces) {
+    if (family == 0) return std::make_tuple(0, tc_npad(std::min(columns, 128)), pieces);
+    const int c = std::min(columns, 64);
+    return std::make_tuple(1, c > 32 ? 64 : (c > 16 ? 32 : (c > 8 ? 16 : 8)), 0);
+}
+
 // Autotuning is allowed on an eager, unprofiled stream.
 bool can_tune(const bie_geom* g, cudaStream_t s) {
     if (!g->autotune || g->prof_on) return false;
@@ -311,7 +321,7 @@ Split direct_sum(bie_geom* g, Kern kind, const double* X, int ldx, int k, const 
         // CTAs about twice the source splits of a full wave: measured faster than the model
         // matched to 64-target CTAs at three per SM)
         const Split base = choose_split(g->n, g->n, g->sms, 2);
-        const auto key = std::make_tuple(1, std::min(k, 64), 0);
+        const auto key = tune_key(1, k, 0);
         auto it = g->tuned.find(key);
         if (it == g->tuned.end() && can_tune(g, s)) {
             std::vector<bie_geom::Tuned> cands{{base.nsplit, base.chunk, 3, 0.0}};
@@ -405,7 +415,7 @@ Split direct_sum_tc(bie_geom* g, const double* X, int k, const double* pre, int 
                             g->bpack.as<uint8_t>(), g->errflag.as<int>(), pieces, ctas, s);
         }
     };
-    const auto key = std::make_tuple(0, kc0, pieces);
+    const auto key = tune_key(0, kc0, pieces);
     auto it = g->tuned.find(key);
     if (it == g->tuned.end() && can_tune(g, s)) {
         std::vector<bie_geom::Tuned> cands;
@@ -923,7 +933,7 @@ bie_geom* geom_create(const double* pts, const double* nrm, const double* w, con
 }
 
 bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, int* ctas, double* ms) {
-    auto it = g->tuned.find(std::make_tuple(family, columns, pieces));
+    auto it = g->tuned.find(tune_key(family, columns, family == 0 ? pieces : 0));
     if (it == g->tuned.end()) return false;
     *nsplit = it->second.nsplit;
     *ctas = it->second.ctas;

@@ -293,7 +293,9 @@ int bie_profile_read(bie_geom* g, int kind, bie_kernel_time* out);
  * tensor-core block sum (columns = min(k, 128), pieces 2 or 3), 1 = FP64 tensor-core
  * sum (columns = min(k, 64), pieces 0). The library times a few candidate launch
  * shapes (CTA shape, source split count) on the first application of each family and
- * column width and keeps the fastest (environment variable BIE_NO_AUTOTUNE turns this
+ * kernel instance (widths rounded up to a multiple of 16 for family 0, to 8, 16, 32 or 64
+ * for family 1, so every width of an instance reads the same entry) and keeps the
+ * fastest (environment variable BIE_NO_AUTOTUNE turns this
  * off). Returns BIE_EINVAL when nothing was tuned for the key. No counterpart in the
  * reference (its FMM has no launch shapes). */
 int bie_tuning_read(bie_geom* g, int32_t family, int32_t columns, int32_t pieces, int32_t* nsplit,

@@ -229,6 +229,14 @@ def test_autotuned_launch_recorded_and_accurate(bie, cfg1, rng):
     assert t_64 is not None and t_64["nsplit"] >= 1
     assert rel(Y64, A @ X + Cm @ X) < 1e-13
     assert rel(Y3, Y64) < 5e-5
+    # widths of the same kernel instance share the entry: 17..32 columns run the 32-wide
+    # tensor-core and FP64 instances tuned above, and reading them retunes nothing
+    for kk in (17, 31, 32):
+        assert bie.tuned_launch(op, "tensor_core", kk) == t_tc
+        assert bie.tuned_launch(op, "fp64", kk) == t_64
+    X2 = rng.standard_normal((itf.n, 19))
+    assert rel(op.mul(X2, precision="bf16x3"), op.mul(X2)) < 5e-5
+    assert bie.tuned_launch(op, "tensor_core", 19) == t_tc
 
 
 def test_workspace_trim_keeps_results(bie, cfg1, monkeypatch):
