@@ -207,6 +207,9 @@ class DielectricInterface:
     def geom(self, near: Optional["_Near"], device: int = 0) -> "_Geom":
         key = (id(near) if near is not None else None, device)
         if key not in self._geoms:
+            if near is not None and near.released:
+                raise RuntimeError("the near-field blocks' host values were released (keep_host_blocks=False); "
+                                   "a geometry on another device needs them: build that operator first")
             self._geoms[key] = _Geom(self, near, device)
         return self._geoms[key]
 
@@ -297,15 +300,33 @@ class _Near:
         self.upsample = {(int(i), int(j)): int(p) for i, j, p in zip(ui, uj, up)}
         self.adaptive = {(int(i), int(j)): ad for i, j in zip(ai, aj)}
         self.n = itf.n
+        self.values_geom = None  # set once the host values are released: the geometry holding them
+
+    @property
+    def released(self) -> bool:
+        return self.values_geom is not None
+
+    def release_host_values(self, geom: "_Geom"):
+        """Frees the library's host copy of the block values (``bie_near_release_values``);
+        ``geom``, a device geometry built from these blocks, holds them from then on and
+        ``val`` reads them back from it."""
+        if self.released:
+            return
+        check(lib().bie_near_release_values(self._h))
+        self.values_geom = geom
 
     @property
     def val(self) -> np.ndarray:
         """Correction block values (nblocks x nb x nb, each block column-major), copied out
-        of the library on first use; a geometry that is only solved on the device never
-        holds a second host copy of its blocks."""
+        of the library on first use (out of the device geometry once the host copy was
+        released); a geometry that is only solved on the device never holds a second host
+        copy of its blocks."""
         if self._val is None:
             v = np.zeros(self.nblocks * self.nb * self.nb)
-            check(lib().bie_near_copy(self._h, None, None, dptr(v), None, None, None, None, None))
+            if self.released:
+                check(lib().bie_geom_near_values(self.values_geom._h, dptr(v), v.size))
+            else:
+                check(lib().bie_near_copy(self._h, None, None, dptr(v), None, None, None, None, None))
             self._val = v
         return self._val
 
@@ -384,13 +405,16 @@ class GPUDielectricOperator:
 
     def __init__(self, interface: DielectricInterface, *, precision: str = "fp64", corrections: bool = True,
                  up_tol: float = 1e-9, max_order: int = 8, correct_edges: bool = True,
-                 adaptive_cfg: Optional[AdaptiveConfig] = None, device: int = 0):
+                 adaptive_cfg: Optional[AdaptiveConfig] = None, device: int = 0, keep_host_blocks: bool = True):
         if precision not in _abi.PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_abi.PRECISIONS)}")
         self.interface = interface
         self.precision = precision
         self.near = interface.near(max_order, up_tol, correct_edges, adaptive_cfg) if corrections else None
         self.geom = interface.geom(self.near, device)
+        if self.near is not None and not keep_host_blocks:
+            # the blocks live on the device only (a server's many resident geometries)
+            self.near.release_host_values(self.geom)
         self.n = interface.n
         self.shape = (self.n, self.n)
         self.dtype = np.float64
@@ -446,12 +470,15 @@ def lhs_dielectric_box3d_fmm3d_corrected(interface: DielectricInterface, fmm_tol
                                          max_order: int, *, correct_edges: bool = True,
                                          adaptive_atol: Optional[float] = None, adaptive_rtol: float = SQRT_EPS,
                                          adaptive_n_GL: int = 0, adaptive_max_depth: int = 20,
-                                         precision: str = "fp64", device: int = 0):
-    """``lhs_dielectric_box3d_fmm3d_corrected`` (src/solver/dielectric_box3d.jl:48-92)."""
+                                         precision: str = "fp64", device: int = 0, keep_host_blocks: bool = True):
+    """``lhs_dielectric_box3d_fmm3d_corrected`` (src/solver/dielectric_box3d.jl:48-92).
+    keep_host_blocks=False frees the host copy of the correction blocks once they are on the
+    device (they are read back from there on request)."""
     ad = AdaptiveConfig(up_tol if adaptive_atol is None else adaptive_atol, adaptive_rtol, adaptive_n_GL,
                         adaptive_max_depth)
     return GPUDielectricOperator(interface, precision=precision, corrections=True, up_tol=up_tol,
-                                 max_order=max_order, correct_edges=correct_edges, adaptive_cfg=ad, device=device)
+                                 max_order=max_order, correct_edges=correct_edges, adaptive_cfg=ad, device=device,
+                                 keep_host_blocks=keep_host_blocks)
 
 
 def batched_lhs_dielectric_box3d_fmm3d_corrected(interface, fmm_tol, up_tol, max_order, **kw):

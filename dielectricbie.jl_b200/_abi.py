@@ -23,7 +23,7 @@ EXPORTS = [
     "bie_last_error", "bie_version", "bie_device_count", "bie_gausslegendre", "bie_best_grid",
     "bie_mesh_single_box", "bie_mesh_multi_box", "bie_mesh_from_panels", "bie_mesh_info", "bie_mesh_copy",
     "bie_mesh_destroy", "bie_near_opts_default", "bie_near_build", "bie_near_info", "bie_near_copy",
-    "bie_near_destroy", "bie_geom_create", "bie_geom_create_from_mesh", "bie_geom_info", "bie_geom_stream",
+    "bie_near_release_values", "bie_near_destroy", "bie_geom_near_values", "bie_geom_create", "bie_geom_create_from_mesh", "bie_geom_info", "bie_geom_stream",
     "bie_geom_destroy", "bie_matvec", "bie_matvec_device", "bie_rhs_point", "bie_rhs_point_device",
     "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve",
     "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
@@ -114,6 +114,8 @@ def lib():
         "bie_near_info": (i, [_vp, C.POINTER(i64), _ip, _ip, _ip, _ip]),
         "bie_near_copy": (i, [_vp, _i32p, _i32p, _dp, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "bie_near_destroy": (None, [_vp]),
+        "bie_near_release_values": (i, [_vp]),
+        "bie_geom_near_values": (i, [_vp, _dp, i64]),
         "bie_geom_create": (i, [_dp, _dp, _dp, _dp, i64, C.c_int32, C.c_int32, _i32p, _i32p, _dp, i64, i,
                                 C.POINTER(_vp)]),
         "bie_geom_create_from_mesh": (i, [_vp, _vp, i, C.POINTER(_vp)]),

@@ -122,6 +122,7 @@ struct bie_mesh {
 };
 struct bie_near {
     bie::Near n;
+    bool values_released = false;
 };
 struct bie_probe {
     bie::ProbeSetup ps;
@@ -288,6 +289,7 @@ int bie_near_copy(const bie_near* nh, int32_t* rowptr, int32_t* col, double* val
                   int32_t* ups_p, int32_t* adp_i, int32_t* adp_j) {
     return guarded([&] {
         REQUIRE(nh, "null near");
+        REQUIRE(!(val && nh->values_released), "near_copy: the block values were released (bie_near_release_values)");
         const bie::Near& n = nh->n;
         if (rowptr) std::copy(n.rowptr.begin(), n.rowptr.end(), rowptr);
         if (col) std::copy(n.col.begin(), n.col.end(), col);
@@ -297,6 +299,14 @@ int bie_near_copy(const bie_near* nh, int32_t* rowptr, int32_t* col, double* val
         if (ups_p) std::copy(n.ups_p.begin(), n.ups_p.end(), ups_p);
         if (adp_i) std::copy(n.adp_i.begin(), n.adp_i.end(), adp_i);
         if (adp_j) std::copy(n.adp_j.begin(), n.adp_j.end(), adp_j);
+    });
+}
+
+int bie_near_release_values(bie_near* n) {
+    return guarded([&] {
+        REQUIRE(n, "null near");
+        std::vector<double>().swap(n->n.val);
+        n->values_released = true;
     });
 }
 
@@ -317,6 +327,7 @@ int bie_geom_create(const double* pts, const double* nrm, const double* w, const
 int bie_geom_create_from_mesh(const bie_mesh* mh, const bie_near* nh, int device, bie_geom** out) {
     return guarded([&] {
         REQUIRE(mh && out, "null argument");
+        REQUIRE(!(nh && nh->values_released), "geom_create_from_mesh: the near-field block values were released");
         const bie::Mesh& m = mh->m;
         const int64_t n = m.npoints();
         REQUIRE(n > 0, "empty mesh");
@@ -341,6 +352,13 @@ int bie_geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes
 }
 
 void* bie_geom_stream(bie_geom* g) { return g ? bie::geom_stream(g) : nullptr; }
+
+int bie_geom_near_values(bie_geom* g, double* val, int64_t len) {
+    return guarded([&] {
+        REQUIRE(g && (val || len == 0), "null argument");
+        REQUIRE(bie::geom_near_values(g, val, len), "geom_near_values: len must be nblocks * nb * nb");
+    });
+}
 
 void bie_geom_destroy(bie_geom* g) {
     if (g) bie::geom_destroy(g);

@@ -1005,6 +1005,16 @@ void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes) {
 
 void* geom_stream(bie_geom* g) { return (void*)g->stream; }
 
+bool geom_near_values(bie_geom* g, double* val, int64_t len) {
+    const int64_t want = g->nblocks * (int64_t)g->nb * g->nb;
+    if (len != want) return false;
+    if (want == 0) return true;
+    DeviceGuard dg(g->device);
+    BIE_CK(cudaMemcpyAsync(val, g->val.p, sizeof(double) * (size_t)want, cudaMemcpyDeviceToHost, g->stream));
+    BIE_CK(cudaStreamSynchronize(g->stream));
+    return true;
+}
+
 void profile_enable(bie_geom* g, int on) {
     DeviceGuard dg(g->device);
     prof_drain(g);

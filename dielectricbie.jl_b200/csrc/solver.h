@@ -44,6 +44,8 @@ void geom_trim(bie_geom* g);
 void geom_trim_if_short(bie_geom* g);
 void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes);
 void* geom_stream(bie_geom* g);
+// Device correction blocks to host (nblocks*nb*nb doubles); false when len differs.
+bool geom_near_values(bie_geom* g, double* val, int64_t len);
 void profile_enable(bie_geom* g, int on);
 void profile_read(bie_geom* g, int kind, bie_kernel_time* out);
 bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, int* ctas, double* ms);

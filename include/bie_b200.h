@@ -121,6 +121,13 @@ int bie_near_info(const bie_near* n, int64_t* nblocks, int* nb, int* n_upsample,
  * source panel i, target panel j, upsampling order p). Any pointer may be NULL. */
 int bie_near_copy(const bie_near* n, int32_t* rowptr, int32_t* col, double* val, int32_t* ups_i, int32_t* ups_j,
                   int32_t* ups_p, int32_t* adp_i, int32_t* adp_j);
+/* Frees the handle's host copy of the block values (nblocks*nb*nb doubles) once a device
+ * geometry holds them; the structure (rowptr, col, pair lists) stays. Afterwards
+ * bie_near_copy with val != NULL and bie_geom_create_from_mesh on this handle return
+ * BIE_EINVAL; bie_geom_near_values reads the values back from a geometry. A server that
+ * keeps many geometries resident holds their blocks once, on the device. No counterpart
+ * in the reference (its operator closure keeps the CSC matrix). */
+int bie_near_release_values(bie_near* n);
 void bie_near_destroy(bie_near* n);
 
 /* ------------------------------------------------------------------------- */
@@ -137,6 +144,9 @@ int bie_geom_create(const double* pts, const double* nrm, const double* w, const
 /* Convenience: from a mesh and (optional) near-field blocks. */
 int bie_geom_create_from_mesh(const bie_mesh* m, const bie_near* near, int device, bie_geom** out);
 int bie_geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* device_bytes);
+/* Copies the geometry's device correction blocks to val (len = nblocks*nb*nb doubles, the
+ * layout of bie_near_copy); BIE_EINVAL when len differs. */
+int bie_geom_near_values(bie_geom* g, double* val, int64_t len);
 /* The CUDA stream (cudaStream_t) the handle's work is ordered on. */
 void* bie_geom_stream(bie_geom* g);
 void bie_geom_destroy(bie_geom* g);

@@ -95,3 +95,28 @@ def test_correction_blocks_match_oracle(bie, orc):
     assert np.abs(D).max() <= 1e-13 * scale
     # same sparsity (structural blocks of the BSR against the CSC's nonzeros)
     assert set(zip(*C_orc.nonzero())) <= set(zip(*C_lib.nonzero()))
+
+
+def test_near_release_values(bie):
+    """bie_near_release_values frees the host block values and keeps the structure:
+    afterwards copying the values or building a geometry from the handle is refused
+    with BIE_EINVAL (no device is touched)."""
+    import ctypes as C
+    from dielectricbie_jl_b200 import _abi
+    L = _abi.lib()
+    itf = bie.single_dielectric_box3d(*CFG1)
+    nr = itf.near(8, 1e-9, True, setup_device=-1)
+    assert nr.nblocks > 0
+    v = np.zeros(nr.nblocks * nr.nb * nr.nb)
+    assert L.bie_near_copy(nr._h, None, None, _abi.dptr(v), None, None, None, None, None) == _abi.BIE_OK
+    assert np.count_nonzero(v) > 0
+    assert L.bie_near_release_values(nr._h) == _abi.BIE_OK
+    assert L.bie_near_release_values(nr._h) == _abi.BIE_OK  # idempotent
+    assert L.bie_near_copy(nr._h, None, None, _abi.dptr(v), None, None, None, None, None) == _abi.BIE_EINVAL
+    assert "released" in _abi.last_error()
+    rp = np.zeros(itf.npanels + 1, dtype=np.int32)
+    assert L.bie_near_copy(nr._h, _abi.i32ptr(rp), None, None, None, None, None, None, None) == _abi.BIE_OK
+    assert np.array_equal(rp, nr.rowptr)
+    g = C.c_void_p()
+    assert L.bie_geom_create_from_mesh(itf._h, nr._h, 0, C.byref(g)) == _abi.BIE_EINVAL
+    assert not g.value
