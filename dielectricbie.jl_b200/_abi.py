@@ -64,7 +64,7 @@ class ServerCounters(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("batches", C.c_int64),
                 ("merged_requests", C.c_int64), ("queued", C.c_int64), ("inflight", C.c_int),
                 ("peak_inflight", C.c_int), ("hbm_budget", C.c_int64), ("hbm_in_use", C.c_int64),
-                ("hbm_peak", C.c_int64)]
+                ("hbm_peak", C.c_int64), ("workspace_releases", C.c_int64), ("enomem_retries", C.c_int64)]
 
 
 class KernelTime(C.Structure):

@@ -10,7 +10,13 @@
 // launches for all of them. Batches on different geometries run at the same time,
 // each on its geometry's CUDA stream, so their kernels overlap on the GPU; work
 // that arrives while others run is admitted as slots and budget free up
-// (continuous batching). Every column of a block solve runs its own Krylov process,
+// (continuous batching). Admission counts the estimated workspace of the batches in
+// flight against the budget (a fraction of the device memory free when the server is
+// created); a geometry keeps its workspace after a batch only while the budget not held by
+// the other batches in flight is still free on the device, so that retained workspaces of
+// idle geometries do not take memory that admission counts on. A batch whose device
+// allocation fails anyway releases its own workspace, waits until it is the only batch in
+// flight and runs once more. Every column of a block solve runs its own Krylov process,
 // so a request's result does not depend on what it was batched with beyond
 // floating-point rounding.
 #include <cuda_runtime.h>
@@ -113,7 +119,7 @@ bool take_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch, siz
     return false;
 }
 
-void run_batch(std::vector<std::shared_ptr<Request>>& batch) {
+void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
     const auto& r0 = batch.front();
     const int64_t n = r0->n;
     int K = 0;
@@ -133,7 +139,23 @@ void run_batch(std::vector<std::shared_ptr<Request>>& batch) {
     std::string err;
     const auto t_start = Clock::now();
     try {
-        rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+        try {
+            rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+        } catch (const Error& e) {
+            if (e.code != BIE_ENOMEM) throw;
+            // memory held by other batches in flight: release this geometry's workspace,
+            // wait (bounded) until this is the only batch in flight, and run once more
+            geom_trim(r0->g);
+            {
+                std::unique_lock<std::mutex> lk(s->mu);
+                s->cnt.enomem_retries += 1;
+                s->cv_done.wait_for(lk, std::chrono::seconds(300), [&] { return s->inflight <= 1 || s->stop; });
+            }
+            st = bie_stats{};
+            st.col_iterations = col_it.data();
+            st.col_resid = col_res.data();
+            rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+        }
         if (rc != BIE_OK) err = "solver did not converge to the requested tolerance";
     } catch (const Error& e) {
         rc = e.code;
@@ -178,7 +200,20 @@ void worker(bie_server* s) {
             s->cnt.merged_requests += (int64_t)batch.size() - 1;
             s->cnt.peak_inflight = std::max(s->cnt.peak_inflight, s->inflight);
         }
-        run_batch(batch);
+        run_batch(s, batch);
+        // keep the geometry's workspace only while the part of the budget that the other
+        // batches in flight do not hold stays free on the device (before the requests
+        // complete: their caller may destroy the geometry once they are polled)
+        size_t floor_b = 0;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            floor_b = s->budget > s->in_use - fp ? s->budget - (s->in_use - fp) : 0;
+        }
+        bool released = false;
+        try {
+            released = geom_trim_if_below(batch.front()->g, floor_b);
+        } catch (...) {
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
             const auto now = Clock::now();
@@ -190,6 +225,7 @@ void worker(bie_server* s) {
             s->in_use -= fp;
             --s->inflight;
             s->cnt.completed += (int64_t)batch.size();
+            s->cnt.workspace_releases += released ? 1 : 0;
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();

@@ -964,14 +964,17 @@ void geom_trim(bie_geom* g) {
     }
 }
 
-void geom_trim_if_short(bie_geom* g) {
+bool geom_trim_if_below(bie_geom* g, size_t free_floor) {
     DeviceGuard dg(g->device);
     size_t fr = 0, tot = 0;
-    if (std::getenv("BIE_TRIM_WORKSPACE") ||
-        (cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr < tot / 4))
-        geom_trim(g);
+    bool trim = std::getenv("BIE_TRIM_WORKSPACE") != nullptr;
+    if (!trim && cudaMemGetInfo(&fr, &tot) == cudaSuccess) trim = fr < std::max(tot / 4, free_floor);
     cudaGetLastError();
+    if (trim) geom_trim(g);
+    return trim;
 }
+
+void geom_trim_if_short(bie_geom* g) { geom_trim_if_below(g, 0); }
 
 void geom_destroy(bie_geom* g) {
     {

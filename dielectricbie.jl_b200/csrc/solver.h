@@ -42,6 +42,9 @@ void geom_destroy(bie_geom* g);
 // _if_short form does so only when less than a quarter of device memory is free.
 void geom_trim(bie_geom* g);
 void geom_trim_if_short(bie_geom* g);
+// geom_trim when the device has less than max(total / 4, free_floor) bytes free (or with
+// BIE_TRIM_WORKSPACE); returns whether it trimmed.
+bool geom_trim_if_below(bie_geom* g, size_t free_floor);
 void geom_info(const bie_geom* g, int64_t* n, int64_t* nblocks, size_t* bytes);
 void* geom_stream(bie_geom* g);
 // Device correction blocks to host (nblocks*nb*nb doubles); false when len differs.

@@ -346,6 +346,8 @@ typedef struct {
     int64_t submitted, completed, batches, merged_requests, queued;
     int inflight, peak_inflight;
     int64_t hbm_budget, hbm_in_use, hbm_peak; /* bytes of estimated solver workspace */
+    int64_t workspace_releases; /* batches after which their geometry's workspace was released */
+    int64_t enomem_retries;     /* batches retried after a device allocation failed */
 } bie_server_counters;
 
 void bie_server_opts_default(bie_server_opts* o);

@@ -71,3 +71,28 @@ def test_server_rejects_bad_requests(bie, stream):
         with pytest.raises(_abi.BieError):
             srv._shapes[12345] = (ops[0][0].n, 1, True)
             srv.result(12345)  # unknown ticket
+
+
+def test_server_releases_workspace_when_memory_is_promised(bie, stream, monkeypatch):
+    """With the whole free device memory as the budget (the geometries' workspaces
+    released before the server is created), every batch leaves less than the budget free,
+    so the server releases the geometry's workspace after each batch; the next batches
+    reallocate it and give the same sigma. With a small budget nothing is released."""
+    ops, reqs = stream
+    sub = reqs[:6]
+    monkeypatch.setenv("BIE_TRIM_WORKSPACE", "1")  # the reference solves end with no workspace
+    alone = [bie.gpu_solve(ops[gi][1], F, rtol=1e-10, precision="bf16x3")[0] for gi, F in sub]
+    monkeypatch.delenv("BIE_TRIM_WORKSPACE")
+    for frac, expect_release in ((1.0, True), (0.05, False)):
+        with bie.SolveServer(max_slots=2, max_batch_rhs=64, hbm_fraction=frac) as srv:
+            out = []
+            for gi, F in sub:  # one at a time: every request is its own batch
+                out.append(srv.result(srv.submit(ops[gi][1], F, rtol=1e-10, precision="bf16x3")))
+            cnt = srv.counters()
+        assert cnt["batches"] == len(sub) and cnt["enomem_retries"] == 0
+        if expect_release:
+            assert cnt["workspace_releases"] == len(sub)
+        else:
+            assert cnt["workspace_releases"] == 0
+        for ref, (S, st, _) in zip(alone, out):
+            assert st.solved and np.all(rel_cols(S, ref) < TOL)
