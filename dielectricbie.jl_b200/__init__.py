@@ -10,7 +10,7 @@ error behaviour) on top of the C ABI of ``libbie_b200.so``:
              batched_lhs_dielectric_box3d_fmm3d_corrected (GPU operators with mul!/@),
              rhs_dielectric_box3d, laplace3d_pottrg, dielectric_diagonal_scaling,
              laplace3d_pottrg_fmm3d_corrected_hcubature (near-accurate probe potentials)
-  solvers    solve_gmres, solve_dielectric_box3d_block, gpu_solve
+  solvers    solve_gmres, solve_dielectric_box3d_block, gpu_solve, gpu_solve_sources
 
 The mesher and the correction-block setup run on the host (as in the
 reference); the direct sums, the correction apply and the Krylov iterations run
@@ -36,7 +36,7 @@ __all__ = [
     "GPUDielectricOperator", "BatchedDielectricOperator", "lhs_dielectric_box3d", "lhs_dielectric_box3d_fmm3d",
     "lhs_dielectric_box3d_fmm3d_corrected", "batched_lhs_dielectric_box3d_fmm3d_corrected",
     "rhs_dielectric_box3d", "laplace3d_pottrg", "dielectric_diagonal_scaling", "solve_gmres",
-    "solve_dielectric_box3d_block", "gpu_solve", "polarization_energy", "BieError", "NotConverged",
+    "solve_dielectric_box3d_block", "gpu_solve", "gpu_solve_sources", "polarization_energy", "BieError", "NotConverged",
     "laplace3d_pottrg_fmm3d_corrected_hcubature", "ProbePotentialOperator",
 ]
 
@@ -668,18 +668,39 @@ def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float 
     Ff, vec = _as_cols(F, op.n)
     k = Ff.shape[1]
     o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+    S, stats = _run_solve(op, k, raise_on_noconv,
+                          lambda S, st: lib().bie_solve(op.geom._h, dptr(Ff), dptr(S), k, C.byref(o), C.byref(st)))
+    return (S[:, 0] if vec else S), stats
+
+
+def _run_solve(op, k, raise_on_noconv, call):
     ci = np.zeros(k, dtype=np.intc)
     cr = np.zeros(k)
     st = _abi.Stats()
     st.col_iterations = ci.ctypes.data_as(C.POINTER(C.c_int))
     st.col_resid = cr.ctypes.data_as(C.POINTER(C.c_double))
     S = np.zeros((op.n, k), order="F")
-    rc = lib().bie_solve(op.geom._h, dptr(Ff), dptr(S), k, C.byref(o), C.byref(st))
+    rc = call(S, st)
     if rc not in (_abi.BIE_OK, _abi.BIE_ENOCONV) or (rc == _abi.BIE_ENOCONV and raise_on_noconv):
         check(rc)
     stats = SolveStats(st.iterations, st.outer, st.fp64_matvecs, st.lowp_matvecs, bool(st.converged),
                        st.max_rel_resid, st.seconds, ci.copy(), cr.copy())
-    return (S[:, 0] if vec else S), stats
+    return S, stats
+
+
+def gpu_solve_sources(op: GPUDielectricOperator, sources, eps_src, *, rtol: float = 1e-10, atol: float = 0.0,
+                      itmax: int = 500, restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6,
+                      max_outer: int = 8, precondition: bool = False, check_every: int = 1,
+                      raise_on_noconv: bool = False):
+    """rhs_dielectric_box3d for point sources and the block solve in one call (C-ABI
+    ``bie_solve_point``): the right-hand sides are built on the device, so only the sources
+    go to the GPU and only Sigma comes back. Returns (Sigma N x k, SolveStats)."""
+    src, q, eps = _point_sources(sources, eps_src)
+    k = len(q)
+    o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+    return _run_solve(op, k, raise_on_noconv,
+                      lambda S, st: lib().bie_solve_point(op.geom._h, dptr(src), dptr(q), dptr(eps), k, dptr(S),
+                                                          C.byref(o), C.byref(st)))
 
 
 def tuned_launch(op: "GPUDielectricOperator", family: str, k: int, pieces: int = 2):
@@ -797,5 +818,5 @@ def solve_dielectric_box3d_block(interface: DielectricInterface, sources, eps_sr
                                                       device=device)
     if eps_src is None:
         eps_src = float(interface.eps_in[0])
-    F = rhs_dielectric_box3d(interface, list(sources), eps_src, device=device)
-    return gpu_solve(op, F, rtol=rtol, atol=atol, itmax=itmax, precondition=precondition, **kw)
+    return gpu_solve_sources(op, list(sources), eps_src, rtol=rtol, atol=atol, itmax=itmax,
+                             precondition=precondition, **kw)

@@ -25,7 +25,7 @@ EXPORTS = [
     "bie_mesh_destroy", "bie_near_opts_default", "bie_near_build", "bie_near_info", "bie_near_copy",
     "bie_near_release_values", "bie_near_destroy", "bie_geom_near_values", "bie_geom_create", "bie_geom_create_from_mesh", "bie_geom_info", "bie_geom_stream",
     "bie_geom_destroy", "bie_matvec", "bie_matvec_device", "bie_rhs_point", "bie_rhs_point_device",
-    "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve",
+    "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve", "bie_solve_point",
     "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
     "bie_server_opts_default", "bie_server_create", "bie_server_submit", "bie_server_poll",
     "bie_server_counters_read", "bie_server_destroy", "bie_tuning_read", "bie_peak_probe",
@@ -139,6 +139,7 @@ def lib():
         "bie_probe_destroy": (None, [_vp]),
         "bie_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
         "bie_solve": (i, [_vp, _dp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats)]),
+        "bie_solve_point": (i, [_vp, _dp, _dp, _dp, C.c_int32, _dp, C.POINTER(SolveOpts), C.POINTER(Stats)]),
         "bie_solve_device": (i, [_vp, _vp, _vp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats), _vp]),
         "bie_profile_enable": (i, [_vp, i]),
         "bie_profile_read": (i, [_vp, i, C.POINTER(KernelTime)]),

@@ -594,6 +594,18 @@ int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_
     return grc != BIE_OK ? grc : rc;
 }
 
+int bie_solve_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* Sigma,
+                    const bie_solve_opts* o, bie_stats* st) {
+    int rc = BIE_OK;
+    int grc = guarded([&] {
+        REQUIRE(g && src && q && eps_src && Sigma && k >= 1, "solve_point: bad argument");
+        bie_solve_opts d;
+        bie_solve_opts_default(&d);
+        rc = bie::solve_point_host(g, src, q, eps_src, k, Sigma, o ? *o : d, st);
+    });
+    return grc != BIE_OK ? grc : rc;
+}
+
 int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o, bie_stats* st,
                      void* stream) {
     int rc = BIE_OK;

@@ -38,7 +38,12 @@ int g_sms[kMaxDevices] = {};
 
 // Device address of the scratch array and the SM count of the current device,
 // looked up on the first call on that device. In host code g_dt_scratch names a
-// host-side stand-in, so the address comes from cudaGetSymbolAddress.
+// host-side stand-in, so the address comes from cudaGetSymbolAddress. The array is
+// part of the library's device module: with lazy module loading (the CUDA 12 default)
+// the module, and with it the 32 MiB, is committed on the device at this lookup, so
+// the first call must come before a pool allocator reserves the device's memory; with
+// CUDA_MODULE_LOADING=EAGER every context that loads the library holds the 32 MiB from
+// the start, whether or not this entry point is used.
 void scratch_for_current_device(double** ptr, int* sms) {
     int dev = -1;
     BIE_CK(cudaGetDevice(&dev));
@@ -46,7 +51,14 @@ void scratch_for_current_device(double** ptr, int* sms) {
     std::lock_guard<std::mutex> lock(g_setup_mu);
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
-        BIE_CK(cudaGetSymbolAddress(&p, g_dt_scratch));
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_dt_scratch);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            throw Error(BIE_ENOMEM,
+                        "dt_apply_static: the device had no room to load the library's 32 MiB scratch array; make "
+                        "the first call on each device before a pool allocator reserves its memory");
+        }
+        BIE_CK(e);
         int n_sm = 0;
         BIE_CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
         g_sms[dev] = n_sm;
@@ -94,8 +106,10 @@ void dt_apply_static(const double* x, const double* y, const double* z, const do
     g.n = n;
     g.perm = nullptr;  // the FP64 kernel reads targets in node order
 
-    // columns per group and source splits, so that nsplit * n * kc fits the scratch;
-    // splits for about four waves of two 128-target CTAs per SM
+    // columns per group and source splits, so that nsplit * n * kc fits the scratch. The
+    // split count follows the regular FP64 path's base rule (about four waves of 128-target
+    // tiles at two per SM); the kernel's CTAs hold 64 targets at three per SM, so this gives
+    // them about twice the splits of a matched wave model, which measured faster there
     const int kc = (int)std::min<int64_t>({64, (int64_t)k, kScratchDoubles / n});
     const int64_t tiles = (n + 127) / 128;
     const int64_t want = (int64_t)sms * 2 * 4;

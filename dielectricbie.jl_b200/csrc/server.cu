@@ -15,14 +15,17 @@
 // created); a geometry keeps its workspace after a batch only while the budget not held by
 // the other batches in flight is still free on the device, so that retained workspaces of
 // idle geometries do not take memory that admission counts on. A batch whose device
-// allocation fails anyway releases its own workspace, waits until it is the only batch in
-// flight and runs once more. Every column of a block solve runs its own Krylov process,
+// allocation fails anyway releases its own workspace and runs once more when every batch in
+// flight is such a retry; retries run one at a time, and no new batch is admitted while one
+// waits, so two batches that fail together do not wait for each other. Every column of a block solve runs its own Krylov process,
 // so a request's result does not depend on what it was batched with beyond
 // floating-point rounding.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -83,6 +86,9 @@ struct bie_server {
     uint64_t next_ticket = 1;
     bool stop = false;
     int inflight = 0;
+    int retry_waiters = 0;    // batches in flight that released their workspace after ENOMEM
+    std::mutex retry_mu;      // held by the one retry that runs
+    std::atomic<int> inject_enomem{0};  // test hook: the next n solves fail with ENOMEM before any device work
     bie_server_counters cnt{};
     std::vector<std::thread> workers;
 };
@@ -92,6 +98,7 @@ namespace {
 
 // Takes the next admissible batch off the queue (caller holds s->mu).
 bool take_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch, size_t& fp) {
+    if (s->retry_waiters > 0) return false;  // a batch waits to retry after ENOMEM: let it have the device
     for (size_t i = 0; i < s->queue.size(); ++i) {
         const std::shared_ptr<Request> r = s->queue[i];
         if (s->busy.count(r->g)) continue;
@@ -140,16 +147,40 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
     const auto t_start = Clock::now();
     try {
         try {
+            int inj = s->inject_enomem.load();
+            while (inj > 0 && !s->inject_enomem.compare_exchange_weak(inj, inj - 1)) {
+            }
+            if (inj > 0) throw Error(BIE_ENOMEM, "injected allocation failure (test hook)");
             rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
         } catch (const Error& e) {
             if (e.code != BIE_ENOMEM) throw;
-            // memory held by other batches in flight: release this geometry's workspace,
-            // wait (bounded) until this is the only batch in flight, and run once more
+            // memory held by other batches in flight: release this geometry's workspace and
+            // run once more when every batch in flight is a retry like this one (they hold no
+            // workspace). Retries take turns under retry_mu; while any waits, take_batch admits
+            // nothing new, so the running batches drain and the wait ends (bounded at 300 s).
             geom_trim(r0->g);
+            struct Waiting {
+                bie_server* s;
+                explicit Waiting(bie_server* sv) : s(sv) {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    s->retry_waiters += 1;
+                    s->cnt.enomem_retries += 1;
+                }
+                ~Waiting() {
+                    {
+                        std::lock_guard<std::mutex> lk(s->mu);
+                        s->retry_waiters -= 1;
+                    }
+                    s->cv_done.notify_all();
+                    s->cv_work.notify_all();
+                }
+            } waiting(s);
+            s->cv_done.notify_all();  // a retry already waiting may now see only retries in flight
+            std::lock_guard<std::mutex> turn(s->retry_mu);
             {
                 std::unique_lock<std::mutex> lk(s->mu);
-                s->cnt.enomem_retries += 1;
-                s->cv_done.wait_for(lk, std::chrono::seconds(300), [&] { return s->inflight <= 1 || s->stop; });
+                s->cv_done.wait_for(lk, std::chrono::seconds(300),
+                                    [&] { return s->inflight <= s->retry_waiters || s->stop; });
             }
             st = bie_stats{};
             st.col_iterations = col_it.data();
@@ -255,6 +286,7 @@ bie_server* server_create(const bie_server_opts& o) {
     s->opt = o;
     s->budget = (size_t)(o.hbm_fraction * (double)free_b);
     s->cnt.hbm_budget = (int64_t)s->budget;
+    if (const char* inj = std::getenv("BIE_TEST_SERVER_ENOMEM")) s->inject_enomem = std::atoi(inj);
     for (int i = 0; i < o.max_slots; ++i) s->workers.emplace_back(worker, s.get());
     return s.release();
 }

@@ -29,7 +29,7 @@ struct bie_geom {
     bie::Buf x, y, z, nx, ny, nz, w, diag, pinv, perm;
     bie::Buf rowptr, col, val;
     // operator workspace
-    bie::Buf part, small, bpack, errflag, cpart;
+    bie::Buf part, small, bpack, errflag, cpart, srcpack;
     int max_row_blocks = 0;  // longest BSR block row (blocks of one target panel)
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
@@ -1310,6 +1310,41 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             for (int c = 0; c < k; ++c) st->col_resid[c] = rel[c];
     }
     return converged ? BIE_OK : BIE_ENOCONV;
+}
+
+// Right-hand sides of k point sources built on the device (rhs_dielectric_box3d,
+// src/solver/dielectric_box3d.jl:95-104) and solved there (solve_dielectric_box3d_block,
+// src/solver/multi_rhs.jl:270-286): only the 5 k source values go to the device and only
+// Sigma comes back, so F never crosses the host link.
+int solve_point_host(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* Sigma,
+                     const bie_solve_opts& o, bie_stats* st) {
+    DeviceGuard dg(g->device);
+    cudaStream_t s = g->stream;
+    std::vector<double> packed((size_t)5 * k);
+    std::copy(src, src + 3 * k, packed.begin());
+    std::copy(q, q + k, packed.begin() + 3 * k);
+    std::copy(eps, eps + k, packed.begin() + 4 * k);
+    upload(g->srcpack, packed.data(), packed.size(), s);
+    const int64_t nk = g->n * (int64_t)k;
+    g->io_a.ensure(sizeof(double) * nk);
+    g->io_b.ensure(sizeof(double) * nk);
+    g->sol.ensure(sizeof(double) * nk);
+    const double* d = g->srcpack.as<double>();
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_rhs_point<<<grid1(nk), 256, 0, s>>>(gdev(g), d, d + 3 * k, d + 4 * k, k, g->io_b.as<double>());
+    }
+    BIE_CK(cudaGetLastError());
+    int rc = solve_device(g, g->io_b.as<double>(), g->sol.as<double>(), k, o, st, s);
+    {
+        Prof pf(g, BIE_KERNEL_OTHER, s);
+        k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->sol.as<double>(), g->n, k, g->io_a.as<double>());
+    }
+    BIE_CK(cudaGetLastError());
+    BIE_CK(cudaMemcpyAsync(Sigma, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    BIE_CK(cudaStreamSynchronize(s));
+    geom_trim_if_short(g);
+    return rc;
 }
 
 int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_solve_opts& o, bie_stats* st) {

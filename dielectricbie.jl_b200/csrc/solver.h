@@ -77,6 +77,8 @@ void potential_host(bie_geom* g, const double* S, int k, const double* T, int64_
 void potential_device(bie_geom* g, const double* S, int k, const double* T, int64_t M, double* phi, cudaStream_t s);
 void energy_host(bie_geom* g, const double* S, int k, const double* src, const double* q, double* W);
 int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_solve_opts& o, bie_stats* st);
+int solve_point_host(bie_geom* g, const double* src, const double* q, const double* eps, int k, double* Sigma,
+                     const bie_solve_opts& o, bie_stats* st);
 int solve_device(bie_geom* g, const double* dF, double* dSigma, int k, const bie_solve_opts& o, bie_stats* st,
                  cudaStream_t s);
 

@@ -178,7 +178,11 @@ int bie_matvec_device(bie_geom* g, const double* dX, double* dY, int32_t k, int3
  * nz and weights w (n each), X and Y node-major n x k (Y must not overlap X).
  * Limit: n <= 4,194,304 nodes; larger n is rejected with BIE_EINVAL before any
  * device work. The first call on a device looks up the array's address; make that
- * first call before any stream capture. Calls share the array: every partial a
+ * first call before any stream capture. Under lazy module loading (the CUDA 12
+ * default) that lookup is also when the 32 MiB is committed on the device: make the
+ * first call before a pool allocator reserves the device's memory, else it fails with
+ * BIE_ENOMEM. With CUDA_MODULE_LOADING=EAGER every context that loads the library
+ * holds the 32 MiB from the start, whether or not this entry point is used. Calls share the array: every partial a
  * call reads is written earlier in the same call, so nothing needs clearing, but
  * calls that overlap on the GPU (other streams, other threads) race on it and
  * must be serialised by the caller. Work is ordered on `stream` (NULL = the
@@ -272,6 +276,14 @@ typedef struct {
 int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st);
 int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o,
                      bie_stats* st, void* stream);
+/* Point-source block solve with host buffers: F[:, c] = rhs_dielectric_box3d(itf,
+ * PointSource(src[:, c], q[c]), eps_src[c]) (src/solver/dielectric_box3d.jl:95-104) is built
+ * on the device and solved there as bie_solve does (solve_dielectric_box3d_block,
+ * src/solver/multi_rhs.jl:270-286). src 3 x k, Sigma N x k (host, column-major). Only the
+ * 5 k source values go to the device and only Sigma comes back: the N x k right-hand side
+ * never crosses the host link, as it does with bie_rhs_point followed by bie_solve. */
+int bie_solve_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* Sigma,
+                    const bie_solve_opts* o, bie_stats* st);
 
 /* ------------------------------------------------------------------------- */
 /* Kernel timing (CUDA events on the launching stream)                        */

@@ -96,3 +96,29 @@ def test_server_releases_workspace_when_memory_is_promised(bie, stream, monkeypa
             assert cnt["workspace_releases"] == 0
         for ref, (S, st, _) in zip(alone, out):
             assert st.solved and np.all(rel_cols(S, ref) < TOL)
+
+
+def test_server_concurrent_enomem_retries_complete_promptly(bie, stream, monkeypatch):
+    """Two batches on different geometries whose first solve fails with ENOMEM (host-side
+    injection before any device work: the environment variable BIE_TEST_SERVER_ENOMEM makes
+    the server's next n solves fail) both release their workspace and retry, one after the
+    other, instead of each waiting for the other to finish; both complete promptly with the
+    same sigma as alone."""
+    import time
+    ops, reqs = stream
+    first = {}
+    for gi, F in reqs:
+        first.setdefault(gi, F)
+    pair = sorted(first.items())[:2]
+    alone = [bie.gpu_solve(ops[gi][1], F, rtol=1e-10, precision="bf16x3")[0] for gi, F in pair]
+    monkeypatch.setenv("BIE_TEST_SERVER_ENOMEM", "2")
+    t0 = time.perf_counter()
+    with bie.SolveServer(max_slots=2, max_batch_rhs=64) as srv:
+        tickets = [srv.submit(ops[gi][1], F, rtol=1e-10, precision="bf16x3") for gi, F in pair]
+        out = [srv.result(t) for t in tickets]
+        cnt = srv.counters()
+    elapsed = time.perf_counter() - t0
+    assert cnt["enomem_retries"] == 2 and cnt["completed"] == 2
+    assert elapsed < 60.0, elapsed  # the old rule waited for the other retry: 300 s
+    for ref, (S, st, _) in zip(alone, out):
+        assert st.solved and np.all(rel_cols(S, ref) < TOL)

@@ -42,14 +42,20 @@ def test_static_entry_rejects_bad_sizes_before_device_work(bie):
     assert rc == _abi.BIE_EINVAL
 
 
+# the small box, and a 94,752-node box on which the scratch bound limits the column group
+# (4,194,304 / n = 44 < 64 columns, so 70 columns run as 44 + 26) and the source splits (1)
+BOXES = [CFG1, (2.0, 1.0, 1.0, 6, 0.05, 10.0, 1.0)]
+
+
 @pytest.mark.gpu
-def test_static_entry_matches_matvec_device_on_consecutive_calls(bie):
+@pytest.mark.parametrize("box", BOXES)
+def test_static_entry_matches_matvec_device_on_consecutive_calls(bie, box):
     import torch
     from dielectricbie_jl_b200 import _abi
     L = _abi.lib()
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
-    itf = bie.single_dielectric_box3d(*CFG1)
+    itf = bie.single_dielectric_box3d(*box)
     n = itf.n
     op = bie.lhs_dielectric_box3d(itf)  # regular path: geometry handle with its own buffers
     g = op.geom._h
@@ -74,6 +80,11 @@ def test_static_entry_matches_matvec_device_on_consecutive_calls(bie):
         _abi.check(L.bie_matvec_device(g, C.c_void_p(X.data_ptr()), C.c_void_p(Y_ref.data_ptr()), k,
                                        _abi.BIE_FP64, flags, None))
         torch.cuda.synchronize()
+        # a repeated call allocates nothing: the device's free memory is unchanged
+        free0 = torch.cuda.mem_get_info(dev)[0]
+        _abi.check(_static_call(L, cols, n, C.c_void_p(X.data_ptr()), k, C.c_void_p(Y_static.data_ptr())))
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info(dev)[0] == free0
         a, b = Y_static.cpu().numpy(), Y_ref.cpu().numpy()
         assert np.isfinite(a).all()
         err = np.linalg.norm(a - b) / np.linalg.norm(b)
