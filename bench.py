@@ -44,15 +44,18 @@ WORKLOADS = {
                  up_tol=1e-9, max_order=8, probes=0, charges="one"),
     # serving stream of uneven geometries (sides U[0.5, 2], eps_in log-U[2, 80], n_quad 4 or 6, node
     # counts log-U[n_min, n_max], geometry repeats with p = 0.5, 1-32 point sources per request)
-    "cfg4": dict(requests=120, n_min=2000, n_max=30000, repeat=0.5, rate=200.0, seed=4, rtol=1e-8,
-                 up_tol=1e-9, max_order=8, k=0),
+    "cfg4": dict(requests=2000, n_min=2000, n_max=200000, repeat=0.5, rate=20.0, seed=4, rtol=1e-8,
+                 up_tol=1e-9, max_order=8, k=0, restart=60),
 }
 
 # lattice of 4 x 4 x 2 cubes (side 0.5, gap 0.2), 16 sources at cell-corner centres between cubes
 WORKLOADS["cfg5"] = dict(lattice=(4, 4, 2), side=0.5, gap=0.2, nq=6, l_ec=0.05, eps_in=4.0, eps_out=1.0, k=16,
                          seed=5, rtol=1e-8, up_tol=1e-9, max_order=8)
 
-SERVE_CFG3 = dict(requests=192, rate=2000.0)  # single-source requests on the cfg3 box
+# serving stream: single-source requests spread over three resident geometries (the cfg3
+# box and two other boxes), Poisson arrivals
+SERVE_STREAM = dict(requests=1024, rate=1500.0, repeats=2,
+                    extra_boxes=[(1.2, 1.0, 0.6, 6, 0.08, 10.0, 1.0), (1.0, 1.0, 0.5, 4, 0.06, 20.0, 1.0)])
 
 
 def load_package():
@@ -243,10 +246,17 @@ def poisson_arrivals(rng, count, rate):
     return np.cumsum(rng.exponential(1.0 / rate, size=count)) - 0.0
 
 
-def serve_stream(bie, requests, precision, rtol, slots=4, batch=128):
-    """Serves `requests` = [(op, F, arrival_s)] through the library's request server
-    (continuous batching), submitting each at its arrival time from a separate thread.
-    Latency = completion - arrival; throughput = RHS columns / (last completion - first arrival)."""
+def rhs_columns(rhs):
+    """Columns of a request's right-hand side: an N x k block, or ("point", sources, eps_src)."""
+    return len(rhs[1]) if isinstance(rhs, tuple) else rhs.shape[1]
+
+
+def serve_stream(bie, requests, precision, rtol, slots=4, batch=128, restart=200):
+    """Serves `requests` = [(op, rhs, arrival_s)] through the library's request server
+    (continuous batching), submitting each at its arrival time from a separate thread; rhs is
+    an N x k block or ("point", sources, eps_src) (bie_server_submit_point: only the sources
+    are queued, the right-hand sides are built on the device). Latency = completion -
+    arrival; throughput = RHS columns / (last completion - first arrival)."""
     srv = bie.SolveServer(max_slots=slots, max_batch_rhs=batch)
     nreq = len(requests)
     tickets, sub_t = [None] * nreq, [0.0] * nreq
@@ -254,12 +264,15 @@ def serve_stream(bie, requests, precision, rtol, slots=4, batch=128):
     t0 = time.perf_counter() + 0.01
 
     def submitter():
-        for i, (op, F, arr) in enumerate(requests):
+        for i, (op, rhs, arr) in enumerate(requests):
             dt = t0 + arr - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
             sub_t[i] = time.perf_counter()
-            tickets[i] = srv.submit(op, F, rtol=rtol, precision=precision)
+            if isinstance(rhs, tuple):
+                tickets[i] = srv.submit_sources(op, rhs[1], rhs[2], rtol=rtol, precision=precision, restart=restart)
+            else:
+                tickets[i] = srv.submit(op, rhs, rtol=rtol, precision=precision, restart=restart)
             ready[i].set()
 
     th = threading.Thread(target=submitter)
@@ -267,11 +280,11 @@ def serve_stream(bie, requests, precision, rtol, slots=4, batch=128):
     lat, done, cols, unsolved = [], [], 0, 0
     for i in range(nreq):
         ready[i].wait()
-        S, st, l_ms = srv.result(tickets[i])
+        _, st, l_ms = srv.result(tickets[i], sigma=False)
         t_done = sub_t[i] + l_ms * 1e-3
         done.append(t_done)
         lat.append((t_done - (t0 + requests[i][2])) * 1e3)
-        cols += requests[i][1].shape[1]
+        cols += rhs_columns(requests[i][1])
         unsolved += int(not st.solved)
     th.join()
     cnt = srv.counters()
@@ -283,53 +296,75 @@ def serve_stream(bie, requests, precision, rtol, slots=4, batch=128):
     for i in order:
         if last is None or done[i] - last > 5e-4:
             widths.append(0)
-        widths[-1] += requests[i][1].shape[1]
+        widths[-1] += rhs_columns(requests[i][1])
         last = done[i]
     return {"solves_per_s": cols / span, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "requests": nreq, "solves": cols,
             "unconverged_requests": unsolved, "batches": cnt["batches"], "merged_requests": cnt["merged_requests"],
-            "batch_columns": widths, "peak_inflight": cnt["peak_inflight"], "hbm_peak_bytes": cnt["hbm_peak"]}
+            "batch_columns": widths if len(widths) <= 64 else f"{len(widths)} completion groups",
+            "peak_inflight": cnt["peak_inflight"], "hbm_peak_bytes": cnt["hbm_peak"],
+            "workspace_releases": cnt["workspace_releases"], "enomem_retries": cnt["enomem_retries"],
+            "group_solves": cnt["groups"], "grouped_batches": cnt["grouped_batches"]}
 
 
-def plain_sequential(bie, requests, rtol):
+def plain_sequential(bie, requests, rtol, restart=200):
     """The plain FP64 GPU path one request at a time in arrival order (a request starts when
-    it has arrived and the previous one is done); same host API and copies as the server."""
+    it has arrived and the previous one is done); same host API as the server's requests
+    (point-source requests through bie_solve_point, blocks through bie_solve)."""
     t_free, lat, cols = 0.0, [], 0
-    for op, F, arr in requests:
+    for op, rhs, arr in requests:
         start = max(arr, t_free)
         t1 = time.perf_counter()
-        bie.gpu_solve(op, F, rtol=rtol, precision="fp64")
+        if isinstance(rhs, tuple):
+            bie.gpu_solve_sources(op, rhs[1], rhs[2], rtol=rtol, precision="fp64", restart=restart)
+        else:
+            bie.gpu_solve(op, rhs, rtol=rtol, precision="fp64", restart=restart)
         t_free = start + (time.perf_counter() - t1)
         lat.append((t_free - arr) * 1e3)
-        cols += F.shape[1]
+        cols += rhs_columns(rhs)
     span = t_free - requests[0][2]
     return {"solves_per_s": cols / span, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span, "requests": len(requests), "solves": cols}
 
 
-def cfg3_request_stream(bie, itf, op, wl, precision):
-    """Single-point-source requests on the cfg3 box, Poisson arrivals (seeded). An untimed
-    warm-up stream of other requests (another seed) goes through a server first, as warm-up
-    steps precede the block solves: it meets the batch widths' first-use costs (launch-shape
-    tuning per kernel instance, workspace growth)."""
-    cnt, rate = SERVE_CFG3["requests"], SERVE_CFG3["rate"]
-    half = np.array(wl["box"]) / 2 * 0.9
+def request_stream(bie, itf, op, wl, precision, device):
+    """Single-point-source requests over three resident geometries (the workload's box and
+    two other boxes of 23k-24k nodes, their correction blocks on the device), Poisson
+    arrivals (seeded). An untimed warm-up stream (another seed) goes through a server first,
+    as warm-up steps precede the block solves: it meets the batch widths' first-use costs
+    (launch-shape tuning per kernel instance, workspace growth). The timed stream is served
+    `repeats` times (the spread of the figures between the runs is reported), then solved
+    by the plain FP64 path one request at a time."""
+    cnt, rate = SERVE_STREAM["requests"], SERVE_STREAM["rate"]
+    geoms = [(itf, op, wl["eps_in"], np.array(wl["box"]) / 2 * 0.9)]
+    for b in SERVE_STREAM["extra_boxes"]:
+        it2 = bie.single_dielectric_box3d(*b)
+        op2 = bie.lhs_dielectric_box3d_fmm3d_corrected(it2, 1e-12, wl["up_tol"], wl["max_order"], precision=precision,
+                                                       device=device, keep_host_blocks=False)
+        geoms.append((it2, op2, b[5], np.array(b[:3]) / 2 * 0.9))
 
     def stream(seed):
         rng = np.random.default_rng(seed)
         arr = poisson_arrivals(rng, cnt, rate)
         reqs = []
         for i in range(cnt):
+            g_itf, g_op, eps, half = geoms[int(rng.integers(len(geoms)))]
             src = bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal()))
-            reqs.append((op, bie.rhs_dielectric_box3d(itf, [src], wl["eps_in"]), float(arr[i])))
+            reqs.append((g_op, ("point", [src], eps), float(arr[i])))
         return reqs
 
     serve_stream(bie, stream(wl["seed"] + 99), precision, wl["rtol"])
     reqs = stream(wl["seed"] + 100)
-    served = serve_stream(bie, reqs, precision, wl["rtol"])
+    runs = [serve_stream(bie, reqs, precision, wl["rtol"]) for _ in range(SERVE_STREAM["repeats"])]
     plain = plain_sequential(bie, reqs, wl["rtol"])
-    return {"workload": f"cfg3 request stream: {cnt} single-source requests, Poisson arrivals at {rate:g}/s "
-                        f"(seeded), rtol {wl['rtol']:g}, after one untimed warm-up stream",
+    sps = [r["solves_per_s"] for r in runs]
+    served = dict(runs[0])
+    served["repeats"] = [{k: r[k] for k in ("solves_per_s", "p50_ms", "p99_ms", "makespan_s", "peak_inflight",
+                                            "batches")} for r in runs]
+    served["solves_per_s_spread"] = (max(sps) - min(sps)) / max(sps)
+    return {"workload": f"request stream: {cnt} single-source requests over {len(geoms)} resident geometries "
+                        f"(N = {', '.join(str(g[0].n) for g in geoms)}), Poisson arrivals at {rate:g}/s (seeded), "
+                        f"rtol {wl['rtol']:g}, after one untimed warm-up stream; served {len(runs)} times",
             "refined_served": served, "plain_fp64_sequential": plain,
             "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"]}
 
@@ -355,10 +390,12 @@ def box_for_nodes(bie, sides, nq, eps_in, target):
 def run_serving_workload(args, wl, bie, device):
     """`--workload cfg4`: the uneven serving stream; served refined solver vs the plain FP64
     path one request at a time. Geometries (mesh + near-field blocks) are built before the
-    timed stream and stay resident, their correction blocks on the device only."""
+    timed stream and stay resident, their correction blocks on the device only; requests
+    carry their point sources only (the right-hand sides are built on the device), so the
+    host holds no N x k blocks."""
     import resource
     rng = np.random.default_rng(wl["seed"])
-    geoms, reqs = [], []
+    geoms, reqs, setup_s = [], [], []
     t_setup = time.perf_counter()
     arr = poisson_arrivals(rng, wl["requests"], wl["rate"])
     for i in range(wl["requests"]):
@@ -369,35 +406,47 @@ def run_serving_workload(args, wl, bie, device):
             eps_in = float(math.exp(rng.uniform(math.log(2.0), math.log(80.0))))
             nq = int(rng.choice([4, 6]))
             target = math.exp(rng.uniform(math.log(wl["n_min"]), math.log(wl["n_max"])))
+            t1 = time.perf_counter()
             itf = box_for_nodes(bie, sides, nq, eps_in, target)
             op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, wl["up_tol"], wl["max_order"], device=device,
                                                           keep_host_blocks=False)
+            setup_s.append((itf.n, time.perf_counter() - t1))
             geoms.append((itf, op, eps_in))
         k = int(rng.integers(1, 33))
         half = 0.45 * (itf.corners.max(axis=(0, 1)) - itf.corners.min(axis=(0, 1)))
         src = [bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal())) for _ in range(k)]
-        reqs.append((op, bie.rhs_dielectric_box3d(itf, src, eps_in), float(arr[i])))
-    setup_s = time.perf_counter() - t_setup
-    # warm-up: one solve per geometry on each path (device buffers, kernel attributes)
+        reqs.append((op, ("point", src, eps_in), float(arr[i])))
+    setup_total = time.perf_counter() - t_setup
+    # warm-up: one cheap solve per geometry on each path (device buffers, kernel attributes,
+    # launch-shape tuning)
+    t_warm = time.perf_counter()
     for itf, op, eps_in in geoms:
-        F = np.ones((itf.n, 1))
-        bie.gpu_solve(op, F, rtol=1e-4, precision=args.precision)
-        bie.gpu_solve(op, F, rtol=1e-4, precision="fp64")
-    served = serve_stream(bie, reqs, args.precision, wl["rtol"])
-    plain = plain_sequential(bie, reqs, wl["rtol"])
+        src = [bie.PointSource((0.0, 0.0, 0.0), 1.0)] * 16
+        bie.gpu_solve_sources(op, src, eps_in, rtol=1e-3, precision=args.precision, restart=wl["restart"])
+        bie.gpu_solve_sources(op, src[:1], eps_in, rtol=1e-3, precision="fp64", restart=wl["restart"])
+    warm_s = time.perf_counter() - t_warm
+    served = serve_stream(bie, reqs, args.precision, wl["rtol"], restart=wl["restart"])
+    plain = plain_sequential(bie, reqs, wl["rtol"], restart=wl["restart"])
     nodes = [itf.n for itf, _, _ in geoms]
+    sn = np.array(setup_s)
     line = {"metric": METRIC, "value": served["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
             "steps": wl["requests"], "warmup": len(geoms), "ms_per_step": served["makespan_s"] * 1e3 / wl["requests"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": f"{args.precision} tensor-core direct sum + fp64",
             "data": "synthetic (seeded boxes and point sources, Poisson arrivals)",
-            "config": {"workload": f"cfg4 serving stream (reduced): {wl['requests']} requests, node counts log-uniform "
+            "config": {"workload": f"cfg4 serving stream: {wl['requests']} requests, node counts log-uniform "
                                    f"in [{wl['n_min']}, {wl['n_max']}], {len(geoms)} distinct geometries "
                                    f"(repeat p = {wl['repeat']}), 1-32 point sources each, Poisson arrivals "
-                                   f"{wl['rate']:g}/s, rtol {wl['rtol']:g}",
-                       "nodes_min": min(nodes), "nodes_max": max(nodes), "geometries": len(geoms),
-                       "geometry_setup": "mesh + near-field blocks built on the host before the timed stream",
-                       "geometry_setup_s": setup_s,
+                                   f"{wl['rate']:g}/s, rtol {wl['rtol']:g}, Krylov restart {wl['restart']}",
+                       "nodes_min": min(nodes), "nodes_max": max(nodes), "nodes_median": float(np.median(nodes)),
+                       "geometries": len(geoms),
+                       "geometry_setup": "mesh + near-field blocks (touching-pair moment sums on the GPU) built "
+                                         "before the timed stream; blocks kept on the device only",
+                       "geometry_setup_s": setup_total,
+                       "geometry_setup_s_per_geometry": {"median": float(np.median(sn[:, 1])),
+                                                         "max": float(sn[:, 1].max()),
+                                                         "at_max_nodes": float(sn[np.argmax(sn[:, 0]), 1])},
+                       "warmup_s": warm_s,
                        "host_peak_rss_gb": resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 2**20},
             "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
             "refined_served": served, "plain_fp64_sequential": plain,
@@ -536,13 +585,14 @@ def main():
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-serving", action="store_true", help="skip the cfg3 request-stream measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the request-stream measurement")
     ap.add_argument("--profile-matvec", action="store_true",
                     help="apply the refined and the FP64 operator once each to k columns and exit "
                          "(small case for ncu captures)")
     ap.add_argument("--columns", type=int, default=0, help="--profile-matvec: columns (default: the workload's k)")
-    ap.add_argument("--cfg4-requests", type=int, default=0, help="--workload cfg4: requests (default 120)")
-    ap.add_argument("--cfg4-nmax", type=int, default=0, help="--workload cfg4: largest node count (default 30000)")
+    ap.add_argument("--cfg4-requests", type=int, default=0, help="--workload cfg4: requests (default 2000)")
+    ap.add_argument("--cfg4-nmax", type=int, default=0, help="--workload cfg4: largest node count (default 200000)")
+    ap.add_argument("--cfg4-rate", type=float, default=0.0, help="--workload cfg4: arrivals per second (default 20)")
     ap.add_argument("--peaks", action="store_true",
                     help="measure the arithmetic ceilings of the direct sums (FP32 FMA, packed FP32 FMA, "
                          "MUFU rsqrt, FP64 FMA, FP64 tensor-core MMA, FP32 -> bf16x2 conversion) on this "
@@ -577,6 +627,8 @@ def main():
             wl["requests"] = args.cfg4_requests
         if args.cfg4_nmax:
             wl["n_max"] = args.cfg4_nmax
+        if args.cfg4_rate:
+            wl["rate"] = args.cfg4_rate
         return run_serving_workload(args, wl, bie, device)
     if args.workload == "cfg5":
         return run_lattice_workload(args, wl, bie, device)
@@ -782,7 +834,7 @@ def main():
     # ---------------- serving: cfg3 request stream, continuous batching vs plain ------
     serving = None
     if args.workload == "cfg3" and world == 1 and not args.no_serving:
-        serving = cfg3_request_stream(bie, itf, op, wl, args.precision)
+        serving = request_stream(bie, itf, op, wl, args.precision, device)
 
     # ---------------- roofline of the dominant kernel ------------------------------
     peaks = {}

@@ -293,14 +293,33 @@ class _Near:
         self.rowptr = np.zeros(itf.npanels + 1, dtype=np.int32)
         self.col = np.zeros(self.nblocks, dtype=np.int32)
         self._val = None  # the block values stay in the library's copy until asked for
-        ui, uj, up = (np.zeros(nu.value, dtype=np.int32) for _ in range(3))
-        ai, aj = (np.zeros(na.value, dtype=np.int32) for _ in range(2))
-        check(lib().bie_near_copy(h, i32ptr(self.rowptr), i32ptr(self.col), None, i32ptr(ui), i32ptr(uj),
-                                  i32ptr(up), i32ptr(ai), i32ptr(aj)))
-        self.upsample = {(int(i), int(j)): int(p) for i, j, p in zip(ui, uj, up)}
-        self.adaptive = {(int(i), int(j)): ad for i, j in zip(ai, aj)}
+        check(lib().bie_near_copy(h, i32ptr(self.rowptr), i32ptr(self.col), None, None, None, None, None, None))
+        self._npairs = (nu.value, na.value)
+        self._ad = ad
+        self._pairs = None  # the pair lists, copied out of the library on first use
         self.n = itf.n
         self.values_geom = None  # set once the host values are released: the geometry holding them
+
+    def _pair_lists(self):
+        if self._pairs is None:
+            nu, na = self._npairs
+            ui, uj, up = (np.zeros(nu, dtype=np.int32) for _ in range(3))
+            ai, aj = (np.zeros(na, dtype=np.int32) for _ in range(2))
+            check(lib().bie_near_copy(self._h, None, None, None, i32ptr(ui), i32ptr(uj), i32ptr(up), i32ptr(ai),
+                                      i32ptr(aj)))
+            self._pairs = ({(int(i), int(j)): int(p) for i, j, p in zip(ui, uj, up)},
+                           {(int(i), int(j)): self._ad for i, j in zip(ai, aj)})
+        return self._pairs
+
+    @property
+    def upsample(self) -> dict:
+        """(source panel, target panel) -> upsampling order, 0-based."""
+        return self._pair_lists()[0]
+
+    @property
+    def adaptive(self) -> dict:
+        """(source panel, target panel) -> AdaptiveConfig of the touching pairs, 0-based."""
+        return self._pair_lists()[1]
 
     @property
     def released(self) -> bool:
@@ -726,14 +745,18 @@ class SolveServer:
     once, each on its geometry's stream; queued requests for the same geometry and
     options are merged into one block solve of at most ``max_batch_rhs`` columns;
     admission also respects an HBM budget (``hbm_fraction`` of the free memory).
+    Point-source batches of up to ``max_group`` different geometries (split-BF16 precision)
+    run together as one group solve, their direct sums in one launch per iteration.
     An operator handed to a server must not be used directly until its requests
     have been collected."""
 
-    def __init__(self, *, max_slots: int = 4, max_batch_rhs: int = 128, hbm_fraction: float = 0.8, device: int = 0):
+    def __init__(self, *, max_slots: int = 4, max_batch_rhs: int = 128, hbm_fraction: float = 0.8, device: int = 0,
+                 max_group: int = 8):
         o = _abi.ServerOpts()
         lib().bie_server_opts_default(C.byref(o))
         o.max_slots, o.max_batch_rhs, o.hbm_fraction, o.device = int(max_slots), int(max_batch_rhs), \
             float(hbm_fraction), int(device)
+        o.max_group = int(max_group)
         h = C.c_void_p()
         check(lib().bie_server_create(C.byref(o), C.byref(h)))
         self._h = h
@@ -750,10 +773,27 @@ class SolveServer:
         self._shapes[t.value] = (op.n, k, vec)
         return t.value
 
-    def result(self, ticket: int, timeout_ms: int = -1):
-        """(Sigma, SolveStats, latency_ms) once the request finished, else None after timeout_ms."""
+    def submit_sources(self, op: GPUDielectricOperator, sources, eps_src, *, rtol: float = 1e-10, atol: float = 0.0,
+                       itmax: int = 500, restart: int = 200, precision: Optional[str] = None,
+                       inner_rtol: float = 1e-6, max_outer: int = 8, precondition: bool = False,
+                       check_every: int = 1) -> int:
+        """Queues the block solve of point-source right-hand sides (C-ABI
+        ``bie_server_submit_point``): only the sources are held until the batch runs, which
+        builds the right-hand sides on the device. The result is N x k as for submit()."""
+        src, q, eps = _point_sources(sources, eps_src)
+        k = len(q)
+        o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+        t = C.c_uint64(0)
+        check(lib().bie_server_submit_point(self._h, op.geom._h, dptr(src), dptr(q), dptr(eps), k, C.byref(o),
+                                            C.byref(t)))
+        self._shapes[t.value] = (op.n, k, False)
+        return t.value
+
+    def result(self, ticket: int, timeout_ms: int = -1, *, sigma: bool = True):
+        """(Sigma, SolveStats, latency_ms) once the request finished, else None after timeout_ms.
+        sigma=False leaves Sigma out (None): the server drops it, nothing N x k is copied."""
         n, k, vec = self._shapes[ticket]
-        S = np.zeros((n, k), order="F")
+        S = np.zeros((n, k), order="F") if sigma else None
         ci = np.zeros(k, dtype=np.intc)
         cr = np.zeros(k)
         st = _abi.Stats()
@@ -761,8 +801,8 @@ class SolveServer:
         st.col_resid = cr.ctypes.data_as(C.POINTER(C.c_double))
         lat = C.c_double(0.0)
         done = C.c_int(0)
-        rc = lib().bie_server_poll(self._h, ticket, int(timeout_ms), dptr(S), C.byref(st), C.byref(lat),
-                                   C.byref(done))
+        rc = lib().bie_server_poll(self._h, ticket, int(timeout_ms), dptr(S) if S is not None else None,
+                                   C.byref(st), C.byref(lat), C.byref(done))
         if rc not in (_abi.BIE_OK, _abi.BIE_ENOCONV):
             del self._shapes[ticket]
             check(rc)
@@ -771,6 +811,8 @@ class SolveServer:
         del self._shapes[ticket]
         stats = SolveStats(st.iterations, st.outer, st.fp64_matvecs, st.lowp_matvecs, rc == _abi.BIE_OK,
                            st.max_rel_resid, st.seconds, ci, cr)
+        if S is None:
+            return None, stats, lat.value
         return (S[:, 0] if vec else S), stats, lat.value
 
     def counters(self) -> dict:

@@ -26,8 +26,10 @@ EXPORTS = [
     "bie_near_release_values", "bie_near_destroy", "bie_geom_near_values", "bie_geom_create", "bie_geom_create_from_mesh", "bie_geom_info", "bie_geom_stream",
     "bie_geom_destroy", "bie_matvec", "bie_matvec_device", "bie_rhs_point", "bie_rhs_point_device",
     "bie_potential", "bie_potential_device", "bie_energy", "bie_solve_opts_default", "bie_solve", "bie_solve_point",
+    "bie_matvec_group_device", "bie_solve_group_device",
     "bie_solve_device", "bie_profile_enable", "bie_profile_read", "bie_dt_apply_static",
-    "bie_server_opts_default", "bie_server_create", "bie_server_submit", "bie_server_poll",
+    "bie_server_opts_default", "bie_server_create", "bie_server_submit", "bie_server_submit_point",
+    "bie_server_poll",
     "bie_server_counters_read", "bie_server_destroy", "bie_tuning_read", "bie_peak_probe",
     "bie_probe_create", "bie_probe_info", "bie_probe_copy", "bie_probe_apply", "bie_probe_destroy",
 ]
@@ -57,14 +59,15 @@ class SolveOpts(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("max_slots", C.c_int), ("max_batch_rhs", C.c_int), ("hbm_fraction", C.c_double),
-                ("device", C.c_int)]
+                ("device", C.c_int), ("max_group", C.c_int)]
 
 
 class ServerCounters(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("batches", C.c_int64),
                 ("merged_requests", C.c_int64), ("queued", C.c_int64), ("inflight", C.c_int),
                 ("peak_inflight", C.c_int), ("hbm_budget", C.c_int64), ("hbm_in_use", C.c_int64),
-                ("hbm_peak", C.c_int64), ("workspace_releases", C.c_int64), ("enomem_retries", C.c_int64)]
+                ("hbm_peak", C.c_int64), ("workspace_releases", C.c_int64), ("enomem_retries", C.c_int64),
+                ("groups", C.c_int64), ("grouped_batches", C.c_int64)]
 
 
 class KernelTime(C.Structure):
@@ -140,6 +143,10 @@ def lib():
         "bie_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
         "bie_solve": (i, [_vp, _dp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats)]),
         "bie_solve_point": (i, [_vp, _dp, _dp, _dp, C.c_int32, _dp, C.POINTER(SolveOpts), C.POINTER(Stats)]),
+        "bie_matvec_group_device": (i, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp), C.POINTER(_vp),
+                                        C.POINTER(C.c_int32), C.c_int32, C.c_uint32, _vp]),
+        "bie_solve_group_device": (i, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp), C.POINTER(_vp),
+                                       C.POINTER(C.c_int32), C.POINTER(SolveOpts), C.POINTER(Stats), _vp]),
         "bie_solve_device": (i, [_vp, _vp, _vp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(Stats), _vp]),
         "bie_profile_enable": (i, [_vp, i]),
         "bie_profile_read": (i, [_vp, i, C.POINTER(KernelTime)]),
@@ -147,6 +154,7 @@ def lib():
         "bie_server_opts_default": (None, [C.POINTER(ServerOpts)]),
         "bie_server_create": (i, [C.POINTER(ServerOpts), C.POINTER(_vp)]),
         "bie_server_submit": (i, [_vp, _vp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(C.c_uint64)]),
+        "bie_server_submit_point": (i, [_vp, _vp, _dp, _dp, _dp, C.c_int32, C.POINTER(SolveOpts), C.POINTER(C.c_uint64)]),
         "bie_server_poll": (i, [_vp, C.c_uint64, C.c_int32, _dp, C.POINTER(Stats), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int)]),
         "bie_server_counters_read": (i, [_vp, C.POINTER(ServerCounters)]),

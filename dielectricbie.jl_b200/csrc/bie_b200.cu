@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <tuple>
 #include <new>
@@ -69,12 +70,15 @@ int occupancy(const void* f, int threads, size_t smem) {
     return occ;
 }
 
+std::atomic<uint64_t> g_alloc_epoch{0};
+
 void Buf::ensure(size_t need) {
     if (need <= bytes) return;
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
     size_t want = need + need / 4 + 256;
+    g_alloc_epoch.fetch_add(1);
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -84,10 +88,14 @@ void Buf::ensure(size_t need) {
     bytes = want;
 }
 void Buf::release() {
-    if (p) cudaFree(p);
+    if (p) {
+        cudaFree(p);
+        g_alloc_epoch.fetch_add(1);
+    }
     p = nullptr;
     bytes = 0;
 }
+uint64_t alloc_epoch() { return g_alloc_epoch.load(); }
 }  // namespace bie
 
 using bie::Error;
@@ -412,6 +420,7 @@ void bie_server_opts_default(bie_server_opts* o) {
     o->max_batch_rhs = 128;
     o->hbm_fraction = 0.8;
     o->device = 0;
+    o->max_group = 8;
 }
 
 int bie_server_create(const bie_server_opts* o, bie_server** out) {
@@ -430,6 +439,16 @@ int bie_server_submit(bie_server* s, bie_geom* g, const double* F, int32_t k, co
         bie_solve_opts d;
         bie_solve_opts_default(&d);
         *ticket = bie::server_submit(s, g, F, k, o ? *o : d);
+    });
+}
+
+int bie_server_submit_point(bie_server* s, bie_geom* g, const double* src, const double* q, const double* eps_src,
+                            int32_t k, const bie_solve_opts* o, uint64_t* ticket) {
+    return guarded([&] {
+        REQUIRE(s && g && src && q && eps_src && ticket && k >= 1, "server_submit_point: bad argument");
+        bie_solve_opts d;
+        bie_solve_opts_default(&d);
+        *ticket = bie::server_submit_point(s, g, src, q, eps_src, k, o ? *o : d);
     });
 }
 
@@ -590,6 +609,29 @@ int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_
         bie_solve_opts d;
         bie_solve_opts_default(&d);
         rc = bie::solve_host(g, F, Sigma, k, o ? *o : d, st);
+    });
+    return grc != BIE_OK ? grc : rc;
+}
+
+int bie_matvec_group_device(bie_geom* const* gs, int32_t G, const double* const* dX, double* const* dY,
+                            const int32_t* ks, int32_t precision, uint32_t flags, void* stream) {
+    return guarded([&] {
+        REQUIRE(gs && dX && dY && ks && G >= 1 && G <= 4096, "matvec_group_device: bad argument");
+        for (int i = 0; i < G; ++i) REQUIRE(dX[i] && dY[i], "matvec_group_device: null member array");
+        bie::matvec_group_device(gs, G, dX, dY, ks, precision, flags, (cudaStream_t)stream);
+    });
+}
+
+int bie_solve_group_device(bie_geom* const* gs, int32_t G, const double* const* dF, double* const* dSigma,
+                           const int32_t* ks, const bie_solve_opts* o, bie_stats* st, void* stream) {
+    int rc = BIE_OK;
+    int grc = guarded([&] {
+        REQUIRE(gs && dF && dSigma && ks && G >= 1 && G <= 4096, "solve_group_device: bad argument");
+        for (int i = 0; i < G; ++i) REQUIRE(dF[i] && dSigma[i], "solve_group_device: null member array");
+        bie_solve_opts d;
+        bie_solve_opts_default(&d);
+        rc = bie::solve_group(gs, G, dF, dSigma, ks, o ? *o : d, st, (cudaStream_t)stream);
+        for (int i = 0; i < G; ++i) bie::geom_trim_if_short(gs[i]);
     });
     return grc != BIE_OK ? grc : rc;
 }

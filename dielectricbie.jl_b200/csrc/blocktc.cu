@@ -34,6 +34,7 @@
 #include <cuda_bf16.h>
 #include <algorithm>
 #include <cstdlib>
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -79,6 +80,9 @@ struct Params {
     int ldp, c0;
     int* err;
 };
+
+// Shared-memory head holding a CTA's copy of its Params and work item.
+constexpr uint32_t kParamHead = ((uint32_t)sizeof(Params) + 2 * sizeof(int) + 15u) & ~15u;
 
 // OR-reduction of a predicate over the NG generator threads (named barrier 1):
 // also orders their shared-memory accesses like bar.sync.
@@ -285,12 +289,17 @@ __device__ __forceinline__ void gen_row_part(const float* __restrict__ ca, const
     }
 }
 
+// The CTA body: target tile `tile`, source split `split` of the geometry in P. The plain
+// launch (k_dt_tc, grid = tiles x splits) reads P from the kernel parameters; the
+// work-list launch (k_dt_tc_list) runs one item of several geometries' tiles per CTA and
+// reads its P from a copy at the head of the CTA's shared memory.
 template <int NP, int NQ>
-__global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
+__device__ __forceinline__ void tc_body(const Params& P, const int tile, const int split, uint8_t* smem_raw) {
     constexpr int NGEN = ngen<NQ>();
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    // carve-up aligned to 1024 bytes in the shared window (128-byte swizzle atoms)
-    uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    // carve-up aligned to 1024 bytes in the shared window (128-byte swizzle atoms), after
+    // the parameter head
+    uint8_t* const head_end = smem_raw + kParamHead;
+    uint8_t* base = head_end + ((1024u - (smem_u32(head_end) & 1023u)) & 1023u);
     const int npad = P.npad;
     const uint32_t a_bytes = M * 128;          // one piece of the A tile (16 KB)
     const uint32_t b_bytes = (uint32_t)npad * 128;  // one piece of the B tile
@@ -312,8 +321,8 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t n = P.g.n;
-    const int64_t i0 = (int64_t)blockIdx.x * M;
-    const int64_t ch0 = (int64_t)blockIdx.y * P.cps;
+    const int64_t i0 = (int64_t)tile * M;
+    const int64_t ch0 = (int64_t)split * P.cps;
     const int64_t ch1 = min(P.nchunks, ch0 + P.cps);
     const int nch = ch1 > ch0 ? (int)(ch1 - ch0) : 0;
     // tensor memory: two FP32 accumulators (alternating periods) and the running
@@ -457,7 +466,7 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
         ok = !gen_any<NGEN>(!ok);  // every generator warp takes the same branch
         if (ok) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float* out = P.part + ((int64_t)blockIdx.y * n + i) * P.ldp + P.c0;
+            float* out = P.part + ((int64_t)split * n + i) * P.ldp + P.c0;
             for (int c = qt * 16; c < npad; c += 16 * NQ) {
                 float h[16];
                 if (nch > 0) {
@@ -578,6 +587,31 @@ __global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
     }
 }
 
+template <int NP, int NQ>
+__global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ) k_dt_tc(Params P) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    tc_body<NP, NQ>(P, (int)blockIdx.x, (int)blockIdx.y, smem_raw);
+}
+
+// Work-list launch: CTA b runs items[b] = (member, target tile, source split, unused) with
+// the member's parameters plist[member]; one launch covers the tiles of several geometries,
+// each with its own nodes, right-hand-side block, width and partials.
+template <int NP, int NQ>
+__global__ void __launch_bounds__(nthreads<NQ>(), 4 / NQ)
+    k_dt_tc_list(const Params* __restrict__ plist, const int4* __restrict__ items) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    Params* sP = reinterpret_cast<Params*>(smem_raw);
+    int* s_item = reinterpret_cast<int*>(smem_raw + sizeof(Params));
+    if (threadIdx.x == 0) {
+        const int4 it = items[blockIdx.x];
+        *sP = plist[it.x];
+        s_item[0] = it.y;
+        s_item[1] = it.z;
+    }
+    __syncthreads();
+    tc_body<NP, NQ>(*sP, s_item[0], s_item[1], smem_raw);
+}
+
 // Packs Q(j, c) = w_j p_j X[j][c0 + c] as NP bf16 pieces, in the swizzled K-major
 // smem image of each 64-source chunk: [chunk][piece][row c][128 B]. Rows c >= keff
 // and sources j >= n are zero.
@@ -614,7 +648,7 @@ size_t smem_bytes(int npad, int np, int sa, int sb) {
     size_t a = (size_t)sa * np * M * 128, b = (size_t)sb * np * npad * 128;
     size_t c = (size_t)SC * 3 * KC * sizeof(float);
     size_t bars = (2 * SAMAX + 2 * SBMAX + 2 * SC + 5) * sizeof(uint64_t) + 16;
-    return 1024 + a + b + c + bars;
+    return kParamHead + 1024 + a + b + c + bars;
 }
 
 // Ring depths for one CTA per SM: the deepest A ring (<= SAMAX) that fits with a
@@ -667,13 +701,21 @@ void launch_k(const Params& P, dim3 grid, size_t sm, cudaStream_t s) {
 }
 
 template <int NP>
-void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit, int64_t cps,
-               float* part, int ldp, uint8_t* bpack, int* err, int force_ctas, cudaStream_t s) {
+void pack_q(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, uint8_t* bpack,
+            cudaStream_t s) {
     const int npad = ((kc + 15) / 16) * 16;
     const int64_t nchunks = (g.n + KC - 1) / KC;
     const int64_t pk = nchunks * npad * 8;
     k_pack_q<NP><<<(unsigned)((pk + 255) / 256), 256, 0, s>>>(g, X, ldx, c0, kc, pre, npad, nchunks, bpack);
     BIE_CK(cudaGetLastError());
+}
+
+template <int NP>
+void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const double* pre, int nsplit, int64_t cps,
+               float* part, int ldp, uint8_t* bpack, int* err, int force_ctas, cudaStream_t s) {
+    const int npad = ((kc + 15) / 16) * 16;
+    const int64_t nchunks = (g.n + KC - 1) / KC;
+    pack_q<NP>(g, X, ldx, c0, kc, pre, bpack, s);
     Params P;
     P.g = g;
     P.bpack = bpack;
@@ -699,7 +741,72 @@ void launch_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc, const
         launch_k<NP, 4>(P, grid, sh.smem, s);
 }
 
+// Work-list launch over the members' (tile, split) items; the shape (CTAs per SM, rings)
+// is that of the widest member, the others run inside it.
+template <int NP>
+void launch_tc_list(const std::vector<TcMember>& ms, int* err, void* dscratch, size_t scratch_bytes, cudaStream_t s) {
+    int npad_max = 16;
+    for (const auto& m : ms) npad_max = std::max(npad_max, ((m.kc + 15) / 16) * 16);
+    const Shape sh = shape(npad_max, NP);
+    std::vector<Params> ps(ms.size());
+    std::vector<int4> items;
+    // members in the caller's order (largest first), each member's tiles x splits
+    for (size_t m = 0; m < ms.size(); ++m) {
+        const TcMember& t = ms[m];
+        pack_q<NP>(t.g, t.X, t.ldx, t.c0, t.kc, t.pre, t.bpack, s);
+        Params& P = ps[m];
+        P.g = t.g;
+        P.bpack = t.bpack;
+        P.npad = ((t.kc + 15) / 16) * 16;
+        P.keff = t.kc;
+        P.nchunks = (t.g.n + KC - 1) / KC;
+        P.cps = t.cps;
+        P.stall_test = 0;
+        P.wait_limit = kWaitLimit;
+        P.sa = sh.sa;
+        P.sb = sh.sb;
+        P.part = t.part;
+        P.ldp = t.ldp;
+        P.c0 = t.c0;
+        P.err = err;
+        const int tiles = (int)((t.g.n + M - 1) / M);
+        for (int sp = 0; sp < t.nsplit; ++sp)
+            for (int ti = 0; ti < tiles; ++ti) items.push_back(make_int4((int)m, ti, sp, 0));
+    }
+    const size_t need = block_tc_list_bytes((int)ms.size(), (int64_t)items.size());
+    if (need > scratch_bytes) throw Error(BIE_EINVAL, "launch_block_tc_list: work-list buffer too small");
+    uint8_t* d = static_cast<uint8_t*>(dscratch);
+    const size_t poff = 0, ioff = ((sizeof(Params) * ms.size() + 255) / 256) * 256;
+    BIE_CK(cudaMemcpyAsync(d + poff, ps.data(), sizeof(Params) * ps.size(), cudaMemcpyHostToDevice, s));
+    BIE_CK(cudaMemcpyAsync(d + ioff, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, s));
+    // the host vectors are pageable: the copies are staged before cudaMemcpyAsync returns
+    const Params* dp = reinterpret_cast<const Params*>(d + poff);
+    const int4* di = reinterpret_cast<const int4*>(d + ioff);
+    const dim3 grid((unsigned)items.size());
+    if (sh.nq == 2) {
+        ensure_smem_limit((const void*)k_dt_tc_list<NP, 2>, sh.smem);
+        k_dt_tc_list<NP, 2><<<grid, nthreads<2>(), sh.smem, s>>>(dp, di);
+    } else {
+        ensure_smem_limit((const void*)k_dt_tc_list<NP, 4>, sh.smem);
+        k_dt_tc_list<NP, 4><<<grid, nthreads<4>(), sh.smem, s>>>(dp, di);
+    }
+    BIE_CK(cudaGetLastError());
+}
+
 }  // namespace tc
+
+size_t block_tc_list_bytes(int nmembers, int64_t nitems) {
+    return ((sizeof(tc::Params) * (size_t)nmembers + 255) / 256) * 256 + sizeof(int4) * (size_t)nitems;
+}
+
+void launch_block_tc_list(const std::vector<TcMember>& ms, int pieces, int* err, void* dscratch, size_t scratch_bytes,
+                          cudaStream_t s) {
+    if (ms.empty()) return;
+    if (pieces == 3)
+        tc::launch_tc_list<3>(ms, err, dscratch, scratch_bytes, s);
+    else
+        tc::launch_tc_list<2>(ms, err, dscratch, scratch_bytes, s);
+}
 
 int tc_npad(int kc) { return ((kc + 15) / 16) * 16; }
 

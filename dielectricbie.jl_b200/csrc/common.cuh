@@ -1,5 +1,6 @@
 // Device-side types shared by the kernel translation units.
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -63,6 +64,25 @@ void launch_block_tc(const GeomDev& g, const double* X, int ldx, int c0, int kc,
                      int64_t cps, float* part, int ldp, uint8_t* bpack, int* err, int pieces, int force_ctas,
                      cudaStream_t s);
 size_t block_tc_pack_bytes(int64_t n, int kc, int pieces);
+// One geometry's share of a K3 work-list launch: columns [c0, c0 + kc) (kc <= 128) of X,
+// nsplit source splits of cps chunks, partials into part (ldp), Q images into bpack.
+struct TcMember {
+    GeomDev g;
+    const double* X;
+    int ldx, c0, kc;
+    const double* pre;
+    int nsplit;
+    int64_t cps;
+    float* part;
+    int ldp;
+    uint8_t* bpack;
+};
+// K3 over the (target tile, source split) work items of several geometries in one launch
+// (members in the given order, each member's Q packed first); the work list and the
+// members' parameters go to dscratch (block_tc_list_bytes of it).
+void launch_block_tc_list(const std::vector<TcMember>& ms, int pieces, int* err, void* dscratch, size_t scratch_bytes,
+                          cudaStream_t s);
+size_t block_tc_list_bytes(int nmembers, int64_t nitems);
 int block_tc_ctas_per_sm(int kc, int pieces, int force_ctas = 0);
 int tc_npad(int kc);
 // K1 with the FP64 tensor-core contraction (dt64mma.cu), columns [c0, c0 + kc), kc <= 64.

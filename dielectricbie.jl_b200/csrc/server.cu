@@ -50,6 +50,10 @@ struct Request {
     int k = 0;
     bie_solve_opts o{};
     std::vector<double> F, S;  // N x k column-major
+    // point-source request: the sources only (x, y, z per column, charges, eps_src); its
+    // right-hand sides are built on the device when its batch runs
+    bool point = false;
+    std::vector<double> src, q, eps;
     std::vector<int> col_it;
     std::vector<double> col_res;
     bie_stats st{};
@@ -96,24 +100,41 @@ struct bie_server {
 namespace bie {
 namespace {
 
-// Takes the next admissible batch off the queue (caller holds s->mu).
-bool take_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch, size_t& fp) {
+// Geometries of at most this many nodes join group solves: there one geometry's launches do
+// not fill the GPU and per-iteration fixed costs dominate; a larger geometry runs alone.
+constexpr int64_t kGroupMaxNodes = 24576;
+
+// Whether a batch led by request r can join a group solve.
+bool groupable(const Request& r) {
+    return r.point && (r.o.precision == BIE_BF16X3 || r.o.precision == BIE_BF16X6) && !r.o.precondition &&
+           r.n <= kGroupMaxNodes;
+}
+
+// Takes the next admissible batch off the queue (caller holds s->mu): the oldest request
+// whose geometry is idle, merged with later ones for the same geometry and options up to
+// kcap columns. like != null restricts it to batches that may join like's group solve;
+// first says whether the batch would be the slot's first (admitted even over the budget
+// when nothing runs).
+bool take_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch, size_t& fp, const Request* like,
+                int kcap, bool first) {
     if (s->retry_waiters > 0) return false;  // a batch waits to retry after ENOMEM: let it have the device
     for (size_t i = 0; i < s->queue.size(); ++i) {
         const std::shared_ptr<Request> r = s->queue[i];
         if (s->busy.count(r->g)) continue;
+        if (like && !(groupable(*r) && same_opts(r->o, like->o))) continue;
+        if (r->k > kcap) continue;
         // gather the oldest request and later ones it can be merged with
         std::vector<size_t> pick{i};
         int K = r->k;
         for (size_t j = i + 1; j < s->queue.size(); ++j) {
             const auto& q = s->queue[j];
-            if (q->g == r->g && same_opts(q->o, r->o) && K + q->k <= s->opt.max_batch_rhs) {
+            if (q->g == r->g && q->point == r->point && same_opts(q->o, r->o) && K + q->k <= kcap) {
                 pick.push_back(j);
                 K += q->k;
             }
         }
         const size_t need = footprint(r->n, K, r->o);
-        if (s->inflight > 0 && s->in_use + need > s->budget) continue;  // admitted later, when memory frees
+        if (!(first && s->inflight == 0) && s->in_use + need > s->budget) continue;  // admitted later
         batch.clear();
         for (size_t j : pick) batch.push_back(s->queue[j]);
         for (size_t t = pick.size(); t-- > 0;) s->queue.erase(s->queue.begin() + (std::ptrdiff_t)pick[t]);
@@ -131,17 +152,30 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
     const int64_t n = r0->n;
     int K = 0;
     for (auto& r : batch) K += r->k;
-    std::vector<double> F((size_t)n * K), S((size_t)n * K);
+    const bool point = r0->point;
+    std::vector<double> F(point ? 0 : (size_t)n * K), S((size_t)n * K);
+    std::vector<double> src(point ? 3 * (size_t)K : 0), q(point ? K : 0), eps(point ? K : 0);
     std::vector<int> col_it(K, 0);
     std::vector<double> col_res(K, 0.0);
     int off = 0;
     for (auto& r : batch) {
-        std::memcpy(F.data() + (size_t)off * n, r->F.data(), sizeof(double) * (size_t)n * r->k);
+        if (point) {
+            std::copy(r->src.begin(), r->src.end(), src.begin() + 3 * (size_t)off);
+            std::copy(r->q.begin(), r->q.end(), q.begin() + off);
+            std::copy(r->eps.begin(), r->eps.end(), eps.begin() + off);
+        } else {
+            std::memcpy(F.data() + (size_t)off * n, r->F.data(), sizeof(double) * (size_t)n * r->k);
+            std::vector<double>().swap(r->F);  // the request's copy is not needed any more
+        }
         off += r->k;
     }
     bie_stats st{};
     st.col_iterations = col_it.data();
     st.col_resid = col_res.data();
+    auto solve = [&]() {
+        return point ? solve_point_host(r0->g, src.data(), q.data(), eps.data(), K, S.data(), r0->o, &st)
+                     : solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+    };
     int rc = BIE_OK;
     std::string err;
     const auto t_start = Clock::now();
@@ -151,7 +185,7 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
             while (inj > 0 && !s->inject_enomem.compare_exchange_weak(inj, inj - 1)) {
             }
             if (inj > 0) throw Error(BIE_ENOMEM, "injected allocation failure (test hook)");
-            rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+            rc = solve();
         } catch (const Error& e) {
             if (e.code != BIE_ENOMEM) throw;
             // memory held by other batches in flight: release this geometry's workspace and
@@ -185,7 +219,7 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
             st = bie_stats{};
             st.col_iterations = col_it.data();
             st.col_resid = col_res.data();
-            rc = solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
+            rc = solve();
         }
         if (rc != BIE_OK) err = "solver did not converge to the requested tolerance";
     } catch (const Error& e) {
@@ -215,48 +249,159 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
     }
 }
 
+// Batches of several geometries solved as one group (solve_group_point_host). If the group
+// runs out of device memory, its members release their workspaces and run one by one
+// (each with run_batch's own retry).
+void run_group(bie_server* s, std::vector<std::vector<std::shared_ptr<Request>>>& group) {
+    const int G = (int)group.size();
+    std::vector<bie_geom*> gs(G);
+    std::vector<int> ks(G, 0);
+    std::vector<std::vector<double>> src(G), q(G), eps(G), S(G), col_res(G);
+    std::vector<std::vector<int>> col_it(G);
+    std::vector<bie_stats> st(G);
+    std::vector<const double*> ps(G), pq(G), pe(G);
+    std::vector<double*> pS(G);
+    for (int m = 0; m < G; ++m) {
+        gs[m] = group[m].front()->g;
+        for (auto& r : group[m]) {
+            ks[m] += r->k;
+            src[m].insert(src[m].end(), r->src.begin(), r->src.end());
+            q[m].insert(q[m].end(), r->q.begin(), r->q.end());
+            eps[m].insert(eps[m].end(), r->eps.begin(), r->eps.end());
+        }
+        S[m].assign((size_t)group[m].front()->n * ks[m], 0.0);
+        col_it[m].assign(ks[m], 0);
+        col_res[m].assign(ks[m], 0.0);
+        st[m] = bie_stats{};
+        st[m].col_iterations = col_it[m].data();
+        st[m].col_resid = col_res[m].data();
+        ps[m] = src[m].data();
+        pq[m] = q[m].data();
+        pe[m] = eps[m].data();
+        pS[m] = S[m].data();
+    }
+    int rc = BIE_OK;
+    std::string err;
+    const auto t_start = Clock::now();
+    try {
+        rc = solve_group_point_host(gs.data(), G, ps.data(), pq.data(), pe.data(), ks.data(), pS.data(),
+                                    group.front().front()->o, st.data());
+        if (rc != BIE_OK) err = "solver did not converge to the requested tolerance";
+    } catch (const Error& e) {
+        if (e.code == BIE_ENOMEM) {
+            for (bie_geom* g : gs) {
+                try {
+                    geom_trim(g);
+                } catch (...) {
+                }
+            }
+            for (auto& b : group) run_batch(s, b);
+            return;
+        }
+        rc = e.code;
+        err = e.what();
+    } catch (const std::exception& e) {
+        rc = BIE_EINVAL;
+        err = e.what();
+    }
+    for (int m = 0; m < G; ++m) {
+        const int64_t n = group[m].front()->n;
+        int off = 0;
+        for (auto& r : group[m]) {
+            r->t_start = t_start;
+            if (rc == BIE_OK || rc == BIE_ENOCONV) {
+                r->S.assign(S[m].begin() + (size_t)off * n, S[m].begin() + (size_t)(off + r->k) * n);
+                r->col_it.assign(col_it[m].begin() + off, col_it[m].begin() + off + r->k);
+                r->col_res.assign(col_res[m].begin() + off, col_res[m].begin() + off + r->k);
+            }
+            r->st = st[m];
+            r->st.col_iterations = nullptr;
+            r->st.col_resid = nullptr;
+            double mx = 0.0;
+            for (double v : r->col_res) mx = std::max(mx, v);
+            r->st.max_rel_resid = mx;
+            // a member's status: the group's ENOCONV applies to the members that missed
+            r->rc = rc == BIE_ENOCONV ? (st[m].converged ? BIE_OK : BIE_ENOCONV) : rc;
+            r->err = r->rc == BIE_OK ? std::string() : err;
+            off += r->k;
+        }
+    }
+}
+
 void worker(bie_server* s) {
     for (;;) {
-        std::vector<std::shared_ptr<Request>> batch;
-        size_t fp = 0;
+        std::vector<std::vector<std::shared_ptr<Request>>> group;
+        std::vector<size_t> fps;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             for (;;) {
                 if (s->stop) return;
-                if (take_batch(s, batch, fp)) break;
+                std::vector<std::shared_ptr<Request>> batch;
+                size_t fp = 0;
+                if (take_batch(s, batch, fp, nullptr, s->opt.max_batch_rhs, true)) {
+                    group.push_back(std::move(batch));
+                    fps.push_back(fp);
+                    break;
+                }
                 s->cv_work.wait(lk);
             }
+            // further geometries' batches for a group solve
+            const Request& lead = *group.front().front();
+            int Klead = 0;
+            for (auto& r : group.front()) Klead += r->k;
+            if (s->opt.max_group > 1 && groupable(lead) && Klead <= 128) {
+                while ((int)group.size() < s->opt.max_group) {
+                    std::vector<std::shared_ptr<Request>> batch;
+                    size_t fp = 0;
+                    if (!take_batch(s, batch, fp, &lead, std::min(128, s->opt.max_batch_rhs), false)) break;
+                    group.push_back(std::move(batch));
+                    fps.push_back(fp);
+                }
+            }
             ++s->inflight;
-            s->cnt.batches += 1;
-            s->cnt.merged_requests += (int64_t)batch.size() - 1;
+            s->cnt.batches += (int64_t)group.size();
+            for (auto& b : group) s->cnt.merged_requests += (int64_t)b.size() - 1;
+            if (group.size() > 1) {
+                s->cnt.groups += 1;
+                s->cnt.grouped_batches += (int64_t)group.size();
+            }
             s->cnt.peak_inflight = std::max(s->cnt.peak_inflight, s->inflight);
         }
-        run_batch(s, batch);
-        // keep the geometry's workspace only while the part of the budget that the other
+        if (group.size() == 1)
+            run_batch(s, group.front());
+        else
+            run_group(s, group);
+        // keep each geometry's workspace only while the part of the budget that the other
         // batches in flight do not hold stays free on the device (before the requests
         // complete: their caller may destroy the geometry once they are polled)
+        size_t fp_all = 0;
+        for (size_t f : fps) fp_all += f;
         size_t floor_b = 0;
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            floor_b = s->budget > s->in_use - fp ? s->budget - (s->in_use - fp) : 0;
+            floor_b = s->budget > s->in_use - fp_all ? s->budget - (s->in_use - fp_all) : 0;
         }
-        bool released = false;
-        try {
-            released = geom_trim_if_below(batch.front()->g, floor_b);
-        } catch (...) {
+        int64_t released = 0;
+        for (auto& b : group) {
+            try {
+                released += geom_trim_if_below(b.front()->g, floor_b) ? 1 : 0;
+            } catch (...) {
+            }
         }
         {
             std::lock_guard<std::mutex> lk(s->mu);
             const auto now = Clock::now();
-            for (auto& r : batch) {
-                r->t_done = now;
-                r->done = true;
+            for (auto& b : group) {
+                for (auto& r : b) {
+                    r->t_done = now;
+                    r->done = true;
+                }
+                s->busy.erase(b.front()->g);
+                s->cnt.completed += (int64_t)b.size();
             }
-            s->busy.erase(batch.front()->g);
-            s->in_use -= fp;
+            s->in_use -= fp_all;
             --s->inflight;
-            s->cnt.completed += (int64_t)batch.size();
-            s->cnt.workspace_releases += released ? 1 : 0;
+            s->cnt.workspace_releases += released;
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();
@@ -267,7 +412,7 @@ void worker(bie_server* s) {
 
 bie_server* server_create(const bie_server_opts& o) {
     if (o.max_slots < 1 || o.max_slots > 64 || o.max_batch_rhs < 1 || o.max_batch_rhs > 256 ||
-        !(o.hbm_fraction > 0.0 && o.hbm_fraction <= 1.0))
+        !(o.hbm_fraction > 0.0 && o.hbm_fraction <= 1.0) || o.max_group < 1 || o.max_group > 64)
         throw Error(BIE_EINVAL, "server_create: bad options");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -301,18 +446,8 @@ void server_destroy(bie_server* s) {
     delete s;
 }
 
-uint64_t server_submit(bie_server* s, bie_geom* g, const double* F, int k, const bie_solve_opts& o) {
-    int64_t n = 0, nblocks = 0;
-    size_t bytes = 0;
-    geom_info(g, &n, &nblocks, &bytes);
-    if (k < 1 || k > s->opt.max_batch_rhs)
-        throw Error(BIE_EINVAL, "server_submit: k must be in [1, max_batch_rhs]");
-    auto r = std::make_shared<Request>();
-    r->g = g;
-    r->n = n;
-    r->k = k;
-    r->o = o;
-    r->F.assign(F, F + (size_t)n * k);
+namespace {
+uint64_t enqueue(bie_server* s, const std::shared_ptr<Request>& r) {
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -324,6 +459,37 @@ uint64_t server_submit(bie_server* s, bie_geom* g, const double* F, int k, const
     }
     s->cv_work.notify_one();
     return r->ticket;
+}
+
+std::shared_ptr<Request> new_request(bie_server* s, bie_geom* g, int k, const bie_solve_opts& o) {
+    int64_t n = 0, nblocks = 0;
+    size_t bytes = 0;
+    geom_info(g, &n, &nblocks, &bytes);
+    if (k < 1 || k > s->opt.max_batch_rhs)
+        throw Error(BIE_EINVAL, "server_submit: k must be in [1, max_batch_rhs]");
+    auto r = std::make_shared<Request>();
+    r->g = g;
+    r->n = n;
+    r->k = k;
+    r->o = o;
+    return r;
+}
+}  // namespace
+
+uint64_t server_submit(bie_server* s, bie_geom* g, const double* F, int k, const bie_solve_opts& o) {
+    auto r = new_request(s, g, k, o);
+    r->F.assign(F, F + (size_t)r->n * k);
+    return enqueue(s, r);
+}
+
+uint64_t server_submit_point(bie_server* s, bie_geom* g, const double* src, const double* q, const double* eps,
+                             int k, const bie_solve_opts& o) {
+    auto r = new_request(s, g, k, o);
+    r->point = true;
+    r->src.assign(src, src + 3 * (size_t)k);
+    r->q.assign(q, q + k);
+    r->eps.assign(eps, eps + k);
+    return enqueue(s, r);
 }
 
 int server_poll(bie_server* s, uint64_t ticket, int timeout_ms, double* Sigma, bie_stats* st, double* latency_ms,

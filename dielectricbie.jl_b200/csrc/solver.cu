@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <mutex>
 #include <memory>
 #include <tuple>
 
@@ -29,7 +30,7 @@ struct bie_geom {
     bie::Buf x, y, z, nx, ny, nz, w, diag, pinv, perm;
     bie::Buf rowptr, col, val;
     // operator workspace
-    bie::Buf part, small, bpack, errflag, cpart, srcpack;
+    bie::Buf part, small, bpack, errflag, cpart, srcpack, glist;
     int max_row_blocks = 0;  // longest BSR block row (blocks of one target panel)
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
@@ -964,12 +965,36 @@ void geom_trim(bie_geom* g) {
     }
 }
 
+// The free-memory query runs only when the library allocated or released device memory
+// since the last query that found enough free memory on this device (for at least this
+// floor): cudaMemGetInfo can take milliseconds, and in steady state (the same solves
+// again, buffers already sized) nothing the library holds has changed.
 bool geom_trim_if_below(bie_geom* g, size_t free_floor) {
     DeviceGuard dg(g->device);
-    size_t fr = 0, tot = 0;
     bool trim = std::getenv("BIE_TRIM_WORKSPACE") != nullptr;
-    if (!trim && cudaMemGetInfo(&fr, &tot) == cudaSuccess) trim = fr < std::max(tot / 4, free_floor);
-    cudaGetLastError();
+    if (!trim) {
+        struct Verdict {
+            uint64_t epoch = ~0ull;
+            size_t floor = 0;
+        };
+        static std::mutex mu;
+        static std::map<int, Verdict> ok;  // per device: last epoch and floor found clear
+        const uint64_t ep = alloc_epoch();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            auto it = ok.find(g->device);
+            if (it != ok.end() && it->second.epoch == ep && free_floor <= it->second.floor) return false;
+        }
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+            trim = fr < std::max(tot / 4, free_floor);
+            if (!trim) {
+                std::lock_guard<std::mutex> lk(mu);
+                ok[g->device] = Verdict{ep, free_floor};
+            }
+        }
+        cudaGetLastError();
+    }
     if (trim) geom_trim(g);
     return trim;
 }
@@ -1368,6 +1393,499 @@ int solve_host(bie_geom* g, const double* F, double* Sigma, int k, const bie_sol
     BIE_CK(cudaMemcpyAsync(Sigma, g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
     BIE_CK(cudaStreamSynchronize(s));
     geom_trim_if_short(g);
+    return rc;
+}
+
+
+// ---------------------------------------------------------------------------
+// Group solves: the block solves of several geometries in lockstep. Every
+// reduced-precision operator application of the group is one work-list launch of the
+// tensor-core direct sum over all members' (target tile, source split) items, followed by
+// each member's correction apply; the Krylov kernels and host checks of all members are
+// issued together on one stream, so a group of small geometries pays one set of
+// per-iteration host round trips instead of one per geometry. The arithmetic of each
+// member is that of its own solve (FP64 refinement around the split-BF16 operator, FP64
+// Krylov), so each result matches the member solved alone within the refined tolerance.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Member {
+    bie_geom* g = nullptr;
+    const double* dF = nullptr;  // node-major n x k
+    double* dX = nullptr;
+    int k = 0;
+    int idx = 0;  // position in the caller's arrays
+    // refinement
+    std::vector<double> fn, tol, rn, eps_in, rel;
+    std::vector<char> act;
+    std::vector<int> col_it;
+    int iters = 0, outer = 0, f64mv = 0, lpmv = 0;
+    bool converged = false, have_true_resid = true;
+    int upd_prec = BIE_FP64;
+    // inner GMRES of the current refinement step
+    const double* dr = nullptr;  // right-hand side of the inner solve
+    double* dx = nullptr;        // its solution
+    std::vector<char> in_act;    // columns the inner solve works on
+    bool cycle = false;          // iterates in the current Arnoldi cycle
+    bool done = false;           // inner solve finished (all columns converged or itmax)
+    int it = 0;                  // inner iterations
+    std::vector<int> gact, jl;
+    std::vector<double> hb;
+};
+
+// Y_m = A_low(X_m) for every member m (split-BF16, pieces 2 or 3): one K3 work-list launch,
+// then each member's corrections and diagonal (combine).
+void group_apply_tc(const std::vector<Member*>& ms, const std::vector<const double*>& X, const std::vector<double*>& Y,
+                    int pieces, uint32_t flags, cudaStream_t s) {
+    if (ms.empty()) return;
+    std::vector<TcMember> tm;
+    std::vector<Split> sp(ms.size());
+    int64_t nitems = 0;
+    for (size_t i = 0; i < ms.size(); ++i) {
+        bie_geom* g = ms[i]->g;
+        const int k = ms[i]->k;
+        sp[i] = tc_split(g, k, pieces);
+        g->part.ensure(sizeof(float) * (size_t)sp[i].nsplit * g->n * k);
+        g->bpack.ensure(block_tc_pack_bytes(g->n, k, pieces));
+        tm.push_back(TcMember{gdev(g), X[i], k, 0, k, nullptr, sp[i].nsplit, sp[i].chunk, g->part.as<float>(), k,
+                              g->bpack.as<uint8_t>()});
+        nitems += ((g->n + kTcTileM - 1) / kTcTileM) * sp[i].nsplit;
+    }
+    bie_geom* lead = ms.front()->g;
+    const size_t need = block_tc_list_bytes((int)ms.size(), nitems);
+    lead->glist.ensure(need);
+    launch_block_tc_list(tm, pieces, lead->errflag.as<int>(), lead->glist.p, lead->glist.bytes, s);
+    for (size_t i = 0; i < ms.size(); ++i) {
+        bie_geom* g = ms[i]->g;
+        const bool corr = g->nblocks > 0 && !(flags & BIE_NO_CORRECTIONS);
+        const bool dg = !(flags & BIE_NO_DIAG);
+        combine(g, g->part.as<float>(), sp[i].nsplit, X[i], Y[i], ms[i]->k, nullptr, corr, dg, s);
+    }
+}
+
+// Copies k values of each member's device array to the host with one synchronisation.
+template <class T, class Get>
+void group_d2h(const std::vector<Member*>& ms, Get get, cudaStream_t s) {
+    for (Member* m : ms) {
+        std::pair<T*, const void*> p = get(m);
+        BIE_CK(cudaMemcpyAsync(p.first, p.second, sizeof(T) * m->k, cudaMemcpyDeviceToHost, s));
+    }
+    BIE_CK(cudaStreamSynchronize(s));
+}
+
+// The inner solve of one refinement step for every member (restarted GMRES, one classical
+// Gram-Schmidt pass: the reduced-precision inner solves stop near 1e-6 and the outer loop
+// recomputes the residual), members in lockstep. Mirrors gmres() without graphs.
+void group_gmres(const std::vector<Member*>& all, int pieces, uint32_t flags, int itmax, int m, int check_every,
+                 cudaStream_t s) {
+    m = std::max(1, std::min(m, itmax));
+    const int m1 = m + 1;
+    for (Member* M : all) {
+        bie_geom* g = M->g;
+        const int64_t nk = g->n * (int64_t)M->k;
+        const int k = M->k;
+        g->V.ensure(sizeof(double) * (size_t)m1 * nk);
+        g->W.ensure(sizeof(double) * nk);
+        g->rr.ensure(sizeof(double) * nk);
+        g->R.ensure(sizeof(double) * (size_t)m1 * m1 * k);
+        g->gv.ensure(sizeof(double) * (size_t)m1 * k);
+        g->cs.ensure(sizeof(double) * (size_t)m1 * k);
+        g->sn.ensure(sizeof(double) * (size_t)m1 * k);
+        g->h.ensure(sizeof(double) * (size_t)m1 * k);
+        g->hn.ensure(sizeof(double) * k);
+        g->beta.ensure(sizeof(double) * k);
+        g->eps.ensure(sizeof(double) * k);
+        g->active.ensure(sizeof(int) * k);
+        g->jlast.ensure(sizeof(int) * k);
+        g->yv.ensure(sizeof(double) * (size_t)m1 * k);
+        g->resid.ensure(sizeof(double) * k);
+        size_t need = 0;
+        for (int nv = 1; nv <= m1; ++nv) {
+            const DotPlan p = dot_plan(g->n, k, nv);
+            need = std::max(need, (size_t)p.nblk * nv * k);
+        }
+        g->dpart.ensure(sizeof(double) * need);
+        BIE_CK(cudaMemsetAsync(M->dx, 0, sizeof(double) * nk, s));
+        upload(g->eps, M->eps_in.data(), k, s);
+        M->it = 0;
+        M->done = false;
+        M->gact.assign(k, 0);
+        M->jl.assign(k, 0);
+        M->hb.assign(k, 0.0);
+    }
+    bool first = true;
+    for (;;) {
+        // residual of the cycle: the right-hand side, or after a restart the true residual
+        // of the current iterate
+        std::vector<Member*> live;
+        for (Member* M : all)
+            if (!M->done) live.push_back(M);
+        if (live.empty()) break;
+        if (!first) {
+            std::vector<const double*> X;
+            std::vector<double*> Y;
+            for (Member* M : live) {
+                X.push_back(M->dx);
+                Y.push_back(M->g->W.as<double>());
+            }
+            group_apply_tc(live, X, Y, pieces, flags, s);
+            for (Member* M : live) {
+                bie_geom* g = M->g;
+                const int64_t nk = g->n * (int64_t)M->k;
+                M->lpmv += 1;
+                BIE_CK(cudaMemcpyAsync(g->rr.p, M->dr, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
+                k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, g->W.as<double>(), 1.0, g->rr.as<double>(), g->n, M->k,
+                                                  nullptr);
+            }
+        }
+        for (Member* M : live) col_norms(M->g, first ? M->dr : M->g->rr.as<double>(), M->k, M->g->beta.as<double>(), s);
+        group_d2h<double>(live, [](Member* M) { return std::make_pair(M->hb.data(), (const void*)M->g->beta.p); }, s);
+        std::vector<Member*> run;
+        for (Member* M : live) {
+            int nact = 0;
+            for (int c = 0; c < M->k; ++c) {
+                M->gact[c] = M->in_act[c] && M->hb[c] > M->eps_in[c] ? 1 : 0;
+                nact += M->gact[c];
+            }
+            if (nact == 0 || M->it >= itmax) {
+                M->done = true;
+                continue;
+            }
+            bie_geom* g = M->g;
+            const int k = M->k;
+            const int64_t nk = g->n * (int64_t)k;
+            upload(g->active, M->gact.data(), k, s);
+            BIE_CK(cudaMemsetAsync(g->jlast.p, 0, sizeof(int) * k, s));
+            BIE_CK(cudaMemsetAsync(g->gv.p, 0, sizeof(double) * m1 * k, s));
+            BIE_CK(cudaMemcpyAsync(g->gv.p, g->beta.p, sizeof(double) * k, cudaMemcpyDeviceToDevice, s));
+            k_scale_cols<<<grid1(nk), 256, 0, s>>>(first ? M->dr : g->rr.as<double>(), g->beta.as<double>(), g->n, k,
+                                                   g->V.as<double>());
+            M->cycle = true;
+            run.push_back(M);
+        }
+        if (run.empty()) break;
+        for (int j = 0; j < m && !run.empty(); ++j) {
+            std::vector<const double*> X;
+            std::vector<double*> Y;
+            for (Member* M : run) {
+                const int64_t nk = M->g->n * (int64_t)M->k;
+                X.push_back(M->g->V.as<double>() + (size_t)j * nk);
+                Y.push_back(M->g->W.as<double>());
+            }
+            group_apply_tc(run, X, Y, pieces, flags, s);
+            for (Member* M : run) {
+                bie_geom* g = M->g;
+                const int k = M->k;
+                const int64_t nk = g->n * (int64_t)k;
+                double* V = g->V.as<double>();
+                double* W = g->W.as<double>();
+                dots(g, V, nk, j + 1, W, k, g->h.as<double>(), 0, s);
+                gs_update_norm(g, W, V, nk, j + 1, g->h.as<double>(), k, g->hn.as<double>(), s);
+                k_scale_cols<<<grid1(nk), 256, 0, s>>>(W, g->hn.as<double>(), g->n, k, V + (size_t)(j + 1) * nk);
+                k_givens<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->h.as<double>(), nullptr, g->hn.as<double>(),
+                                                    g->cs.as<double>(), g->sn.as<double>(), g->gv.as<double>(),
+                                                    g->active.as<int>(), g->jlast.as<int>(), g->eps.as<double>(),
+                                                    g->resid.as<double>(), j, m1, k);
+                BIE_CK(cudaGetLastError());
+                M->lpmv += 1;
+                M->it += 1;
+            }
+            if ((j + 1) % std::max(1, check_every) == 0 || j + 1 == m) {
+                group_d2h<int>(run, [](Member* M) { return std::make_pair(M->gact.data(), (const void*)M->g->active.p); },
+                               s);
+                std::vector<Member*> still;
+                for (Member* M : run) {
+                    bool any = false;
+                    for (int c = 0; c < M->k; ++c) any = any || M->gact[c];
+                    if (any && M->it < itmax) still.push_back(M);
+                }
+                run.swap(still);
+            }
+        }
+        // solution update of every member that iterated in this cycle
+        std::vector<Member*> cyc;
+        for (Member* M : live)
+            if (M->cycle) cyc.push_back(M);
+        for (Member* M : cyc) {
+            bie_geom* g = M->g;
+            const int k = M->k;
+            const int64_t nk = g->n * (int64_t)k;
+            k_backsolve<<<grid1(k, 64), 64, 0, s>>>(g->R.as<double>(), g->gv.as<double>(), g->jlast.as<int>(), m1, k,
+                                                    g->yv.as<double>());
+            k_update_solution<<<grid1(nk), 256, 0, s>>>(M->dx, g->V.as<double>(), nk, g->yv.as<double>(),
+                                                        g->jlast.as<int>(), m, nullptr, g->n, k);
+            BIE_CK(cudaGetLastError());
+        }
+        group_d2h<int>(cyc, [](Member* M) { return std::make_pair(M->jl.data(), (const void*)M->g->jlast.p); }, s);
+        group_d2h<int>(cyc, [](Member* M) { return std::make_pair(M->gact.data(), (const void*)M->g->active.p); }, s);
+        for (Member* M : cyc) {
+            M->cycle = false;
+            for (int c = 0; c < M->k; ++c) M->col_it[c] += M->jl[c];
+            bool any = false;
+            for (int c = 0; c < M->k; ++c) any = any || M->gact[c];
+            if (!any || M->it >= itmax) M->done = true;
+        }
+        first = false;
+    }
+}
+
+}  // namespace
+
+namespace {
+void check_group(bie_geom* const* gs, int G, const int* ks) {
+    if (G < 1) throw Error(BIE_EINVAL, "empty group");
+    for (int i = 0; i < G; ++i) {
+        if (!gs[i] || ks[i] < 1 || ks[i] > 128) throw Error(BIE_EINVAL, "group member needs 1..128 columns");
+        for (int j = 0; j < i; ++j)
+            if (gs[j] == gs[i]) throw Error(BIE_EINVAL, "a geometry appears twice in a group");
+        if (gs[i]->device != gs[0]->device) throw Error(BIE_EINVAL, "group members on different devices");
+    }
+}
+}  // namespace
+
+void matvec_group_device(bie_geom* const* gs, int G, const double* const* dX, double* const* dY, const int* ks,
+                         int prec, uint32_t flags, cudaStream_t s) {
+    check_prec(prec);
+    if (prec != BIE_BF16X3 && prec != BIE_BF16X6)
+        throw Error(BIE_EUNSUPPORTED, "group operator applications run the split-BF16 precisions");
+    check_group(gs, G, ks);
+    DeviceGuard dg(gs[0]->device);
+    if (!s) s = gs[0]->stream;
+    for (int i = 0; i < G; ++i)
+        if (gs[i]->stream != s) BIE_CK(cudaStreamSynchronize(gs[i]->stream));
+    std::vector<Member> mem(G);
+    std::vector<Member*> ms;
+    std::vector<const double*> X;
+    std::vector<double*> Y;
+    for (int i = 0; i < G; ++i) {
+        mem[i].g = gs[i];
+        mem[i].k = ks[i];
+        ms.push_back(&mem[i]);
+    }
+    std::stable_sort(ms.begin(), ms.end(), [](const Member* a, const Member* b) { return a->g->n > b->g->n; });
+    for (Member* M : ms) {
+        const int i = (int)(M - mem.data());
+        X.push_back(dX[i]);
+        Y.push_back(dY[i]);
+    }
+    group_apply_tc(ms, X, Y, prec == BIE_BF16X6 ? 3 : 2, flags, s);
+    for (Member* M : ms) check_device_error(M->g, s);
+}
+
+int solve_group(bie_geom* const* gs, int G, const double* const* dF, double* const* dX, const int* ks,
+                const bie_solve_opts& o, bie_stats* st, cudaStream_t s) {
+    check_prec(o.precision);
+    if (o.precision != BIE_BF16X3 && o.precision != BIE_BF16X6)
+        throw Error(BIE_EUNSUPPORTED, "group solves run the split-BF16 precisions");
+    if (o.precondition) throw Error(BIE_EUNSUPPORTED, "group solves run without the diagonal preconditioner");
+    if (o.itmax < 1 || o.restart < 1 || !(o.rtol >= 0) || !(o.atol >= 0)) throw Error(BIE_EINVAL, "bad solver options");
+    check_group(gs, G, ks);
+    DeviceGuard dg(gs[0]->device);
+    if (!s) s = gs[0]->stream;
+    // the members' own streams finish their work before the group's stream starts
+    for (int i = 0; i < G; ++i)
+        if (gs[i]->stream != s) BIE_CK(cudaStreamSynchronize(gs[i]->stream));
+    const int pieces = o.precision == BIE_BF16X6 ? 3 : 2;
+    const double inner_delta = pieces == 3 ? kDeltaBF16X6 : kDeltaBF16X3;
+    std::vector<Member> mem(G);
+    std::vector<Member*> ms;
+    for (int i = 0; i < G; ++i) {
+        Member& M = mem[i];
+        M.g = gs[i];
+        M.dF = dF[i];
+        M.dX = dX[i];
+        M.k = ks[i];
+        M.idx = i;
+        ms.push_back(&M);
+    }
+    // largest members first: their items lead the work list
+    std::stable_sort(ms.begin(), ms.end(), [](const Member* a, const Member* b) { return a->g->n > b->g->n; });
+    BIE_CK(cudaEventRecord(ms.front()->g->ev0, s));
+    for (Member* M : ms) {
+        bie_geom* g = M->g;
+        const int k = M->k;
+        const int64_t nk = g->n * (int64_t)k;
+        g->small.ensure(sizeof(double) * (size_t)std::max(2 * k, 8));
+        col_norms(g, M->dF, k, g->small.as<double>(), s);
+        g->rr.ensure(sizeof(double) * nk);
+        g->dd.ensure(sizeof(double) * nk);
+        g->xo.ensure(sizeof(double) * nk);
+        BIE_CK(cudaMemsetAsync(M->dX, 0, sizeof(double) * nk, s));
+        BIE_CK(cudaMemcpyAsync(g->xo.p, M->dF, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
+        M->fn.assign(k, 0.0);
+        M->col_it.assign(k, 0);
+        M->rel.assign(k, 0.0);
+        M->act.assign(k, 1);
+        M->eps_in.assign(k, 0.0);
+        M->in_act.assign(k, 1);
+    }
+    group_d2h<double>(ms, [](Member* M) { return std::make_pair(M->fn.data(), (const void*)M->g->small.p); }, s);
+    for (Member* M : ms) {
+        M->tol.resize(M->k);
+        for (int c = 0; c < M->k; ++c) M->tol[c] = o.atol + o.rtol * M->fn[c];
+        M->rn = M->fn;
+    }
+    struct Upd { int prec; double delta; };
+    std::vector<Upd> upd;
+    if (o.precision == BIE_BF16X3) upd.push_back({BIE_BF16X3, kDeltaBF16X3});
+    upd.push_back({BIE_BF16X6, kDeltaBF16X6});
+    for (int it_out = 0;; ++it_out) {
+        std::vector<Member*> act;
+        for (Member* M : ms) {
+            int nact = 0;
+            double worst = 0.0;
+            for (int c = 0; c < M->k; ++c) {
+                M->act[c] = M->rn[c] > M->tol[c] ? 1 : 0;
+                nact += M->act[c];
+                M->rel[c] = M->fn[c] > 0 ? M->rn[c] / M->fn[c] : 0.0;
+                if (M->act[c]) worst = std::max(worst, M->rn[c] / M->tol[c]);
+            }
+            if (nact == 0) {
+                M->converged = true;
+                continue;
+            }
+            if (it_out >= o.max_outer || M->iters >= o.itmax) continue;
+            M->upd_prec = BIE_FP64;
+            for (const Upd& u : upd)
+                if (u.delta * worst <= 0.5) {
+                    M->upd_prec = u.prec;
+                    break;
+                }
+            for (int c = 0; c < M->k; ++c)
+                M->eps_in[c] = std::max({o.inner_rtol * M->rn[c], 0.5 * M->tol[c], 2.0 * inner_delta * M->rn[c]});
+            M->in_act = M->act;
+            M->dr = M->g->xo.as<double>();
+            M->dx = M->g->dd.as<double>();
+            act.push_back(M);
+        }
+        if (act.empty()) break;
+        int budget = o.itmax;
+        for (Member* M : act) budget = std::min(budget, o.itmax - M->iters);
+        group_gmres(act, pieces, o.flags, std::max(1, budget), o.restart, o.check_every, s);
+        // x += d, then the residual update: reduced precision (one work-list launch per
+        // precision) or the FP64 operator
+        std::vector<Member*> low[4];
+        for (Member* M : act) {
+            bie_geom* g = M->g;
+            const int k = M->k;
+            const int64_t nk = g->n * (int64_t)k;
+            M->iters += M->it;
+            upload(g->active, std::vector<int>(M->act.begin(), M->act.end()).data(), k, s);
+            k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, g->dd.as<double>(), 1.0, M->dX, g->n, k, g->active.as<int>());
+            BIE_CK(cudaGetLastError());
+            M->outer += 1;
+            if (M->upd_prec != BIE_FP64) {
+                low[M->upd_prec].push_back(M);
+            } else {
+                apply_op(g, M->dX, g->xo.as<double>(), k, BIE_FP64, o.flags, nullptr, s);
+                M->f64mv += 1;
+                k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, M->dF, -1.0, g->xo.as<double>(), g->n, k, nullptr);
+                M->have_true_resid = true;
+            }
+        }
+        for (int p : {BIE_BF16X3, BIE_BF16X6}) {
+            if (low[p].empty()) continue;
+            std::vector<const double*> X;
+            std::vector<double*> Y;
+            for (Member* M : low[p]) {
+                X.push_back(M->g->dd.as<double>());
+                Y.push_back(M->g->rr.as<double>());
+            }
+            group_apply_tc(low[p], X, Y, p == BIE_BF16X6 ? 3 : 2, o.flags, s);
+            for (Member* M : low[p]) {
+                bie_geom* g = M->g;
+                const int64_t nk = g->n * (int64_t)M->k;
+                M->lpmv += 1;
+                k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, g->rr.as<double>(), 1.0, g->xo.as<double>(), g->n, M->k,
+                                                  nullptr);
+                M->have_true_resid = false;
+            }
+        }
+        for (Member* M : act) col_norms(M->g, M->g->xo.as<double>(), M->k, M->g->small.as<double>(), s);
+        group_d2h<double>(act, [](Member* M) { return std::make_pair(M->rn.data(), (const void*)M->g->small.p); }, s);
+    }
+    const bool verify = !(o.flags & 4u) && (st != nullptr);
+    if (verify) {
+        std::vector<Member*> vm;
+        for (Member* M : ms)
+            if (!M->have_true_resid) vm.push_back(M);
+        for (Member* M : vm) {
+            bie_geom* g = M->g;
+            const int64_t nk = g->n * (int64_t)M->k;
+            apply_op(g, M->dX, g->xo.as<double>(), M->k, BIE_FP64, o.flags, nullptr, s);
+            M->f64mv += 1;
+            k_axpby<<<grid1(nk), 256, 0, s>>>(1.0, M->dF, -1.0, g->xo.as<double>(), g->n, M->k, nullptr);
+            col_norms(g, g->xo.as<double>(), M->k, g->small.as<double>(), s);
+        }
+        group_d2h<double>(vm, [](Member* M) { return std::make_pair(M->rn.data(), (const void*)M->g->small.p); }, s);
+        for (Member* M : vm)
+            for (int c = 0; c < M->k; ++c) M->rel[c] = M->fn[c] > 0 ? M->rn[c] / M->fn[c] : 0.0;
+    }
+    bie_geom* lead = ms.front()->g;
+    BIE_CK(cudaEventRecord(lead->ev1, s));
+    BIE_CK(cudaEventSynchronize(lead->ev1));
+    float msec = 0.f;
+    BIE_CK(cudaEventElapsedTime(&msec, lead->ev0, lead->ev1));
+    bool all = true;
+    for (Member* M : ms) {
+        check_device_error(M->g, s);
+        all = all && M->converged;
+        if (!st) continue;
+        bie_stats& t = st[M->idx];
+        t.iterations = M->iters;
+        t.outer = M->outer;
+        t.fp64_matvecs = M->f64mv;
+        t.lowp_matvecs = M->lpmv;
+        t.converged = M->converged ? 1 : 0;
+        double mx = 0.0;
+        for (int c = 0; c < M->k; ++c) mx = std::max(mx, M->rel[c]);
+        t.max_rel_resid = mx;
+        t.seconds = msec * 1e-3;
+        if (t.col_iterations)
+            for (int c = 0; c < M->k; ++c) t.col_iterations[c] = M->col_it[c];
+        if (t.col_resid)
+            for (int c = 0; c < M->k; ++c) t.col_resid[c] = M->rel[c];
+    }
+    return all ? BIE_OK : BIE_ENOCONV;
+}
+
+int solve_group_point_host(bie_geom* const* gs, int G, const double* const* src, const double* const* q,
+                           const double* const* eps, const int* ks, double* const* Sigma, const bie_solve_opts& o,
+                           bie_stats* st) {
+    check_group(gs, G, ks);
+    DeviceGuard dg(gs[0]->device);
+    cudaStream_t s = gs[0]->stream;
+    std::vector<const double*> dF(G);
+    std::vector<double*> dX(G);
+    for (int i = 0; i < G; ++i) {
+        bie_geom* g = gs[i];
+        const int k = ks[i];
+        const int64_t nk = g->n * (int64_t)k;
+        if (g->stream != s) BIE_CK(cudaStreamSynchronize(g->stream));
+        std::vector<double> packed((size_t)5 * k);
+        std::copy(src[i], src[i] + 3 * k, packed.begin());
+        std::copy(q[i], q[i] + k, packed.begin() + 3 * k);
+        std::copy(eps[i], eps[i] + k, packed.begin() + 4 * k);
+        upload(g->srcpack, packed.data(), packed.size(), s);
+        g->io_a.ensure(sizeof(double) * nk);
+        g->io_b.ensure(sizeof(double) * nk);
+        g->sol.ensure(sizeof(double) * nk);
+        const double* d = g->srcpack.as<double>();
+        k_rhs_point<<<grid1(nk), 256, 0, s>>>(gdev(g), d, d + 3 * k, d + 4 * k, k, g->io_b.as<double>());
+        BIE_CK(cudaGetLastError());
+        dF[i] = g->io_b.as<double>();
+        dX[i] = g->sol.as<double>();
+    }
+    const int rc = solve_group(gs, G, dF.data(), dX.data(), ks, o, st, s);
+    for (int i = 0; i < G; ++i) {
+        bie_geom* g = gs[i];
+        const int64_t nk = g->n * (int64_t)ks[i];
+        k_nodemajor_to_colmajor<<<grid1(nk), 256, 0, s>>>(g->sol.as<double>(), g->n, ks[i], g->io_a.as<double>());
+        BIE_CK(cudaGetLastError());
+        BIE_CK(cudaMemcpyAsync(Sigma[i], g->io_a.p, sizeof(double) * nk, cudaMemcpyDeviceToHost, s));
+    }
+    BIE_CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < G; ++i) geom_trim_if_short(gs[i]);
     return rc;
 }
 

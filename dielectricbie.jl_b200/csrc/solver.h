@@ -24,6 +24,9 @@ void ensure_smem_limit(const void* f, size_t bytes);
 // CTAs per SM of kernel f with `threads` threads and `smem` bytes, cached per device.
 int occupancy(const void* f, int threads, size_t smem);
 
+// Count of the library's device allocations and releases so far (all Buf objects).
+uint64_t alloc_epoch();
+
 // Grow-only device buffer owned by a geometry handle.
 struct Buf {
     void* p = nullptr;
@@ -81,11 +84,26 @@ int solve_point_host(bie_geom* g, const double* src, const double* q, const doub
                      const bie_solve_opts& o, bie_stats* st);
 int solve_device(bie_geom* g, const double* dF, double* dSigma, int k, const bie_solve_opts& o, bie_stats* st,
                  cudaStream_t s);
+// Block solves of G geometries in lockstep (split-BF16 precisions): each reduced-precision
+// operator application is one work-list launch of the tensor-core direct sum over all
+// members. Device arrays node-major; st (if not null) has G entries.
+int solve_group(bie_geom* const* gs, int G, const double* const* dF, double* const* dX, const int* ks,
+                const bie_solve_opts& o, bie_stats* st, cudaStream_t s);
+// Point-source right-hand sides built on the device per member, solved as a group, Sigma
+// copied back per member (host, column-major); the members' k source values in src/q/eps.
+int solve_group_point_host(bie_geom* const* gs, int G, const double* const* src, const double* const* q,
+                           const double* const* eps, const int* ks, double* const* Sigma, const bie_solve_opts& o,
+                           bie_stats* st);
+// Y_m = A_low X_m for every member in one work-list launch of the tensor-core direct sum.
+void matvec_group_device(bie_geom* const* gs, int G, const double* const* dX, double* const* dY, const int* ks,
+                         int prec, uint32_t flags, cudaStream_t s);
 
 // server.cu: request server with continuous batching of block solves.
 bie_server* server_create(const bie_server_opts& o);
 void server_destroy(bie_server* s);
 uint64_t server_submit(bie_server* s, bie_geom* g, const double* F, int k, const bie_solve_opts& o);
+uint64_t server_submit_point(bie_server* s, bie_geom* g, const double* src, const double* q, const double* eps,
+                             int k, const bie_solve_opts& o);
 int server_poll(bie_server* s, uint64_t ticket, int timeout_ms, double* Sigma, bie_stats* st, double* latency_ms,
                 int* done, std::string* err);
 void server_counters(bie_server* s, bie_server_counters* out);

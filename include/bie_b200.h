@@ -272,7 +272,9 @@ typedef struct {
  * workspace, about (restart + 1) N k doubles, when less than a quarter of the device
  * memory is free (always with the environment variable BIE_TRIM_WORKSPACE), so that many
  * resident geometries solved in turn do not keep a workspace each. The next solve
- * allocates it again. */
+ * allocates it again. The free memory is queried only when the library's own device
+ * allocations changed since the last query that found enough free (a steady stream of
+ * solves does not pay for the query). */
 int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st);
 int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, const bie_solve_opts* o,
                      bie_stats* st, void* stream);
@@ -284,6 +286,27 @@ int bie_solve_device(bie_geom* g, const double* dF, double* dSigma, int32_t k, c
  * never crosses the host link, as it does with bie_rhs_point followed by bie_solve. */
 int bie_solve_point(bie_geom* g, const double* src, const double* q, const double* eps_src, int32_t k, double* Sigma,
                     const bie_solve_opts* o, bie_stats* st);
+
+/* Several geometries at once: the reduced-precision operator of G geometries applied in
+ * ONE launch of the tensor-core direct sum over a work list of every geometry's (target tile,
+ * source split) items, largest geometries first, followed by each geometry's correction
+ * apply: mul!(Y, ::BatchedDielectricOperator, X) (src/solver/multi_rhs.jl:103-136) for G
+ * operators of uneven size. precision BIE_BF16X3 or BIE_BF16X6; member i has ks[i] <= 128
+ * columns, dX[i] / dY[i] node-major n_i x k_i device arrays; the geometries must differ and
+ * live on one device. Work is ordered on `stream` (NULL = the first geometry's); the
+ * members' own streams are synchronised first. */
+int bie_matvec_group_device(bie_geom* const* gs, int32_t G, const double* const* dX, double* const* dY,
+                            const int32_t* ks, int32_t precision, uint32_t flags, void* stream);
+/* Block solves of G geometries in lockstep (solve_dielectric_box3d_block per geometry,
+ * src/solver/multi_rhs.jl:270-286), precision BIE_BF16X3 or BIE_BF16X6: every inner Krylov
+ * iteration applies all members' operators with one work-list launch (as
+ * bie_matvec_group_device) and issues their Krylov kernels and convergence reads together,
+ * so a group of small geometries pays one set of per-iteration host round trips. Each
+ * member runs its own FP64 refinement and Krylov processes, as bie_solve_device would; st
+ * (optional) has G entries. The diagonal preconditioner is not available here
+ * (BIE_EUNSUPPORTED). */
+int bie_solve_group_device(bie_geom* const* gs, int32_t G, const double* const* dF, double* const* dSigma,
+                           const int32_t* ks, const bie_solve_opts* o, bie_stats* st, void* stream);
 
 /* ------------------------------------------------------------------------- */
 /* Kernel timing (CUDA events on the launching stream)                        */
@@ -352,6 +375,10 @@ typedef struct {
     int max_batch_rhs;   /* columns merged into one block solve (default 128, <= 256) */
     double hbm_fraction; /* admission budget: this fraction of the device's free memory at creation (0.8) */
     int device;          /* CUDA device of the budget (the geometries carry their own) */
+    int max_group;       /* point-source batches of up to this many different geometries of at most
+                            24,576 nodes (same options, split-BF16 precision, <= 128 columns each) run as
+                            one group solve (bie_solve_group_device) in one slot (default 8; 1 = one
+                            geometry per slot) */
 } bie_server_opts;
 
 typedef struct {
@@ -360,6 +387,8 @@ typedef struct {
     int64_t hbm_budget, hbm_in_use, hbm_peak; /* bytes of estimated solver workspace */
     int64_t workspace_releases; /* batches after which their geometry's workspace was released */
     int64_t enomem_retries;     /* batches retried after a device allocation failed */
+    int64_t groups;             /* group solves (two or more geometries in lockstep) */
+    int64_t grouped_batches;    /* batches that ran inside a group solve */
 } bie_server_counters;
 
 void bie_server_opts_default(bie_server_opts* o);
@@ -367,6 +396,13 @@ int bie_server_create(const bie_server_opts* o, bie_server** out);
 /* Copies F (host, N x k column-major) and queues the solve; *ticket identifies it. */
 int bie_server_submit(bie_server* s, bie_geom* g, const double* F, int32_t k, const bie_solve_opts* o,
                       uint64_t* ticket);
+/* Queues a block solve of point-source right-hand sides, rhs_dielectric_box3d(itf,
+ * PointSource(src[:, c], q[c]), eps_src[c]) (src/solver/dielectric_box3d.jl:95-104): only the
+ * 5 k source values are copied; the right-hand sides are built on the device when the batch
+ * runs (as bie_solve_point does), so a queue of many requests holds no N x k host blocks.
+ * Point-source requests merge with each other, not with bie_server_submit's. src 3 x k. */
+int bie_server_submit_point(bie_server* s, bie_geom* g, const double* src, const double* q, const double* eps_src,
+                            int32_t k, const bie_solve_opts* o, uint64_t* ticket);
 /* Waits up to timeout_ms (< 0: until done) for the request. *done = 1 when finished:
  * Sigma (host N x k, may be NULL), stats and the submit-to-completion latency are
  * filled, the ticket is retired and the solve's status is returned (BIE_ENOCONV

@@ -122,3 +122,44 @@ def test_server_concurrent_enomem_retries_complete_promptly(bie, stream, monkeyp
     assert elapsed < 60.0, elapsed  # the old rule waited for the other retry: 300 s
     for ref, (S, st, _) in zip(alone, out):
         assert st.solved and np.all(rel_cols(S, ref) < TOL)
+
+
+def test_server_point_requests_equal_alone(bie, stream):
+    """Point-source requests (bie_server_submit_point: only the sources are queued, the
+    right-hand sides are built on the device when the batch runs) merge into block solves and
+    give each request's sigma as solved alone (bie_solve_point)."""
+    ops, _ = stream
+    rng = np.random.default_rng(99)
+    reqs = []
+    for _ in range(9):
+        gi = int(rng.integers(len(ops)))
+        itf, op, b = ops[gi]
+        half = 0.4 * np.array(b[:3])
+        k = int(rng.integers(1, 12))
+        reqs.append((gi, [bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal()))
+                          for _ in range(k)], b[5]))
+    alone = [bie.gpu_solve_sources(ops[gi][1], src, eps, rtol=1e-10, precision="bf16x3")[0] for gi, src, eps in reqs]
+    with bie.SolveServer(max_slots=2, max_batch_rhs=64) as srv:
+        tickets = [srv.submit_sources(ops[gi][1], src, eps, rtol=1e-10, precision="bf16x3") for gi, src, eps in reqs]
+        out = [srv.result(t) for t in tickets]
+        cnt = srv.counters()
+    for ref, (S, st, lat) in zip(alone, out):
+        assert st.solved and S.shape == ref.shape
+        assert np.all(rel_cols(S, ref) < TOL)
+    assert cnt["completed"] == len(reqs) and cnt["merged_requests"] > 0
+    # batches of different geometries ran together as group solves (one direct-sum launch
+    # per iteration for all of them)
+    assert cnt["groups"] >= 1 and cnt["grouped_batches"] >= 2
+
+
+def test_server_without_groups_gives_the_same(bie, stream):
+    """max_group = 1 (one geometry per slot) serves the same point requests to the same
+    sigma; no group solve runs."""
+    ops, _ = stream
+    itf, op, b = ops[0]
+    srcs = [bie.PointSource((0.05 * i, -0.02 * i, 0.01), 1.0 - 0.1 * i) for i in range(5)]
+    ref = bie.gpu_solve_sources(op, srcs, b[5], rtol=1e-10, precision="bf16x3")[0]
+    with bie.SolveServer(max_slots=1, max_batch_rhs=64, max_group=1) as srv:
+        S, st, _ = srv.result(srv.submit_sources(op, srcs, b[5], rtol=1e-10, precision="bf16x3"))
+        cnt = srv.counters()
+    assert st.solved and np.all(rel_cols(S, ref) < TOL) and cnt["groups"] == 0
