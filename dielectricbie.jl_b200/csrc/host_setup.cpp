@@ -818,6 +818,9 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
     const bool gpu_adp = o.device >= 0 && nq <= 6;
     struct AdpJob { int j; std::vector<std::array<double, 4>> leaves; };
     std::vector<std::vector<AdpJob>> adp_jobs(gpu_adp ? P : 0);
+    // upsampled blocks of sources whose order is at most 8 run on the GPU too
+    const bool gpu_ups = o.device >= 0 && nq <= 6;
+    std::vector<int> ups_order(P, 0);  // > 0: this source's upsampled blocks go to the GPU
     const int nGL = o.adaptive_n_GL == 0 ? nq : o.adaptive_n_GL;
     int hit_any = 0;
     const double aatol = o.adaptive_atol < 0 ? o.up_tol : o.adaptive_atol;
@@ -835,6 +838,14 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
             per_src[i].push_back(std::move(b));
         };
         if (!ups[i].empty()) {
+            int nup = 0;
+            for (auto& e : ups[i]) nup = std::max(nup, e.second);
+            if (gpu_ups && nup <= 8) {
+                ups_order[i] = nup;
+                nup = 0;  // nothing to do on the host
+            }
+        }
+        if (!ups[i].empty() && ups_order[i] == 0) {
             int nup = 0;
             for (auto& e : ups[i]) nup = std::max(nup, e.second);
             SourceCache sc;
@@ -915,6 +926,47 @@ int near_build(const Mesh& m, const NearOpts& o, Near& out, std::string& err) {
                 for (int s = 0; s < np; ++s)
                     for (int r = 0; r < np; ++r) b.v[(size_t)s * np + r] = Kb[(size_t)r * np + s] - Kd[(size_t)r * np + s];
                 per_src[i].push_back(std::move(b));
+            }
+        }
+    }
+    if (gpu_ups) {
+        // one launch for every source panel with GPU-side upsampled blocks
+        std::vector<int> js, jn, tg;
+        std::vector<double> jf;
+        std::vector<int64_t> toff{0};
+        for (int i = 0; i < P; ++i) {
+            if (!ups_order[i]) continue;
+            js.push_back(i);
+            jn.push_back(ups_order[i]);
+            const PanelFrame& f = fr[i];
+            const double fv[10] = {f.cc.x, f.cc.y, f.cc.z, f.bma.x, f.bma.y, f.bma.z, f.dma.x, f.dma.y, f.dma.z, f.scale};
+            jf.insert(jf.end(), fv, fv + 10);
+            for (auto& e : ups[i]) tg.push_back(e.first);
+            toff.push_back((int64_t)tg.size());
+        }
+        if (!js.empty()) {
+            // Gauss nodes, weights and barycentric rows per order (as source_cache computes them)
+            const int T = 9;
+            std::vector<double> xu((size_t)T * T, 0.0), wu((size_t)T * T, 0.0), ex((size_t)T * T * nq, 0.0);
+            for (int n = 1; n <= 8; ++n) {
+                gauss_legendre(n, xu.data() + (size_t)n * T, wu.data() + (size_t)n * T);
+                for (int a = 0; a < n; ++a)
+                    bary_row(nq, m.glx.data(), m.bary.data(), xu[(size_t)n * T + a], ex.data() + ((size_t)n * T + a) * nq);
+            }
+            std::vector<double> blocks((size_t)tg.size() * np * np);
+            if (upsampled_blocks_gpu(o.device, nq, m.pts.data(), N, m.w.data(), m.normals.data(), P, (int)js.size(),
+                                     js.data(), jn.data(), jf.data(), toff.data(), tg.data(), xu.data(), wu.data(),
+                                     ex.data(), blocks.data(), err) != 0)
+                return -1;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nth)
+#endif
+            for (int q = 0; q < (int)js.size(); ++q) {
+                const int i = js[q];
+                for (int64_t p = toff[q]; p < toff[q + 1]; ++p) {
+                    const double* b = blocks.data() + (size_t)p * np * np;
+                    per_src[i].push_back(Blk{tg[p], i, std::vector<double>(b, b + (size_t)np * np)});
+                }
             }
         }
     }

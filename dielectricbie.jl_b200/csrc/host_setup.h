@@ -48,7 +48,8 @@ struct NearOpts {
     int adaptive_n_GL = 0;
     int adaptive_max_depth = 20;
     int nthreads = 0;
-    int device = -1;  // >= 0: the adaptive blocks' moment sums run on this CUDA device (n_quad <= 6)
+    int device = -1;  // >= 0: the adaptive blocks' moment sums and the upsampled blocks (n_up <= 8)
+                      // run on this CUDA device (n_quad <= 6)
 };
 
 // Moment blocks of the adaptive (touching) pairs on a CUDA device (near_gpu.cu):
@@ -60,6 +61,17 @@ int adaptive_blocks_gpu(int device, int nq, int ngl, const double* glx, const do
                         const double* wg, const double* pts, int64_t npts, const double* normals, int npanels,
                         int npairs, const int* trg, const double* frames, const int64_t* leaf_off,
                         const double* leaves, double* Kb, std::string& err);
+
+// Upsampled blocks on a CUDA device (near_gpu.cu), bitwise equal to the host's: job q is
+// source panel job_src[q] at order job_nup[q] (<= 8) with frame job_frame[10 q ..], its
+// target panels tgt[tgt_off[q] .. tgt_off[q + 1]); xu/wu/ex are the Gauss nodes, weights and
+// barycentric rows of each order n at [n * 9 + i] (ex: [(n * 9 + i) * nq + m]). out receives
+// one nq^2 x nq^2 block per pair in the BSR value layout (column-major), upsampled minus
+// direct. Returns 0, or -1 with err set.
+int upsampled_blocks_gpu(int device, int nq, const double* pts, int64_t npts, const double* w, const double* normals,
+                         int npanels, int njobs, const int* job_src, const int* job_nup, const double* job_frame,
+                         const int64_t* tgt_off, const int* tgt, const double* xu, const double* wu, const double* ex,
+                         double* out, std::string& err);
 
 // Near-field corrections in block-sparse-row form: block rows = target panels,
 // block columns = source panels, each block nb x nb (nb = nq^2) stored

@@ -9,9 +9,21 @@
 // shared memory; each thread then accumulates its (target, basis) outputs over the
 // leaf's quadrature points in the host's order with explicitly rounded operations,
 // so the blocks are bitwise those of the host code (which has no fused multiply-add).
+//
+// Upsampled near-field blocks on the GPU (laplace3d_DT_corrections,
+// src/kernel/laplace3d_near_upsampling.jl:127-270): for source panel i at its upsampling
+// order n_up (the maximum over its neighbours) and each of its target panels j,
+//
+//   block[s][t] = sum_alpha Mt[s][alpha] G_n(p_up[alpha], x_t, n_j) - G_n(y_s, x_t, n_j) w_s
+//
+// with Mt the barycentric-interpolated upsampled quadrature (build_source_cache). One CTA
+// per source panel stages p_up and Mt once, then the kernel values of each target panel;
+// every sum runs in the host's order with explicitly rounded operations, so the blocks are
+// bitwise those of the host code.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -134,7 +146,142 @@ __global__ void __launch_bounds__(256) k_adaptive_blocks(Tables tb, const double
     }
 }
 
+constexpr int kMaxUp = 8;  // upsampling orders handled on the GPU (n_up^2 <= 64 staged points)
+
+// One CTA per job (source panel). job_frame[10 q ..] = (cc, b - a, d - a, scale) of the
+// source; tables per order n (stride kMaxUp + 1): xu[n][i], wu[n][i], ex[n][i][m] (the
+// barycentric rows of the upsampled nodes on the panel's n_quad Gauss nodes). Output:
+// block of pair p = tgt_off[q] + e at out[p * np^2], column-major (s * np + t).
+__global__ void __launch_bounds__(256) k_upsampled_blocks(int nq, const double* __restrict__ pts,
+                                                          const double* __restrict__ w,
+                                                          const double* __restrict__ normals,
+                                                          const int* __restrict__ job_src,
+                                                          const int* __restrict__ job_nup,
+                                                          const double* __restrict__ job_frame,
+                                                          const int64_t* __restrict__ tgt_off,
+                                                          const int* __restrict__ tgt, const double* __restrict__ xu,
+                                                          const double* __restrict__ wu, const double* __restrict__ ex,
+                                                          double* __restrict__ out) {
+    extern __shared__ double sm[];
+    const int q = blockIdx.x;
+    const int np = nq * nq;
+    const int n_up = job_nup[q], nu2 = n_up * n_up;
+    const int src = job_src[q];
+    double* pu = sm;                  // [nu2][3] upsampled source points
+    double* Mt = pu + 3 * nu2;        // [np][nu2]
+    double* km = Mt + (size_t)np * nu2;  // [np][nu2] kernel values at one target panel
+    const double* fr = job_frame + (size_t)q * 10;
+    const double* xn = xu + (size_t)n_up * (kMaxUp + 1);
+    const double* wn = wu + (size_t)n_up * (kMaxUp + 1);
+    const double* en = ex + (size_t)n_up * (kMaxUp + 1) * nq;
+    for (int a = threadIdx.x; a < nu2; a += blockDim.x) {
+        const int i = a / n_up, j = a - i * n_up;
+        const double hi = __ddiv_rn(xn[i], 2.0), hj = __ddiv_rn(xn[j], 2.0);
+        pu[3 * a + 0] = add(add(fr[0], mul(fr[3], hi)), mul(fr[6], hj));
+        pu[3 * a + 1] = add(add(fr[1], mul(fr[4], hi)), mul(fr[7], hj));
+        pu[3 * a + 2] = add(add(fr[2], mul(fr[5], hi)), mul(fr[8], hj));
+    }
+    for (int e = threadIdx.x; e < np * nu2; e += blockDim.x) {
+        const int mm = e / nu2, a = e - mm * nu2;
+        const int mx = mm / nq, my = mm - mx * nq, i = a / n_up, j = a - i * n_up;
+        Mt[e] = mul(mul(mul(mul(fr[9], wn[i]), wn[j]), en[i * nq + mx]), en[j * nq + my]);
+    }
+    for (int64_t p = tgt_off[q]; p < tgt_off[q + 1]; ++p) {
+        const int trg = tgt[p];
+        const V3d nt{normals[3 * trg], normals[3 * trg + 1], normals[3 * trg + 2]};
+        __syncthreads();  // staging done / previous target's values consumed
+        for (int e = threadIdx.x; e < np * nu2; e += blockDim.x) {
+            const int t = e / nu2, a = e - t * nu2;
+            const double* xt = pts + 3 * ((size_t)trg * np + t);
+            km[e] = lap_grad_d(V3d{pu[3 * a], pu[3 * a + 1], pu[3 * a + 2]}, V3d{xt[0], xt[1], xt[2]}, nt);
+        }
+        __syncthreads();
+        double* o = out + (size_t)p * np * np;
+        for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+            const int t = e / np, mm = e - t * np;
+            const double* mt = Mt + (size_t)mm * nu2;
+            const double* kv = km + (size_t)t * nu2;
+            double acc = 0.0;
+            for (int a = 0; a < nu2; ++a) acc = add(acc, mul(mt[a], kv[a]));
+            const size_t js = (size_t)src * np + mm;
+            const double* xt = pts + 3 * ((size_t)trg * np + t);
+            const double kd = mul(lap_grad_d(V3d{pts[3 * js], pts[3 * js + 1], pts[3 * js + 2]},
+                                             V3d{xt[0], xt[1], xt[2]}, nt),
+                                  w[js]);
+            o[(size_t)mm * np + t] = sub(acc, kd);
+        }
+    }
+}
+
 }  // namespace
+
+int upsampled_blocks_gpu(int device, int nq, const double* pts, int64_t npts, const double* w, const double* normals,
+                         int npanels, int njobs, const int* job_src, const int* job_nup, const double* job_frame,
+                         const int64_t* tgt_off, const int* tgt, const double* xu, const double* wu, const double* ex,
+                         double* out, std::string& err) {
+    if (njobs == 0) return 0;
+    if (nq > 6) {
+        err = "upsampled blocks on the GPU support n_quad <= 6";
+        return -1;
+    }
+    int max_up = 0;
+    for (int q = 0; q < njobs; ++q) max_up = std::max(max_up, job_nup[q]);
+    if (max_up > kMaxUp) {
+        err = "upsampled blocks on the GPU support n_up <= 8";
+        return -1;
+    }
+    const int np = nq * nq;
+    const int64_t npairs = tgt_off[njobs];
+    int prev = 0;
+    cudaGetDevice(&prev);
+    std::vector<void*> bufs;
+    auto fail = [&](cudaError_t e, const char* what) {
+        for (void* p : bufs) cudaFree(p);
+        cudaSetDevice(prev);
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        cudaGetLastError();
+        return -1;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+    auto upload = [&](const void* src, size_t bytes, void** dst) -> cudaError_t {
+        cudaError_t r = cudaMalloc(dst, bytes > 0 ? bytes : 8);
+        if (r != cudaSuccess) return r;
+        bufs.push_back(*dst);
+        return bytes ? cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    const size_t tab = (size_t)(kMaxUp + 1) * (kMaxUp + 1);
+    void *d_pts, *d_w, *d_nrm, *d_js, *d_jn, *d_fr, *d_off, *d_tgt, *d_xu, *d_wu, *d_ex, *d_out;
+    if ((e = upload(pts, sizeof(double) * 3 * npts, &d_pts)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(w, sizeof(double) * npts, &d_w)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(normals, sizeof(double) * 3 * npanels, &d_nrm)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(job_src, sizeof(int) * njobs, &d_js)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(job_nup, sizeof(int) * njobs, &d_jn)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(job_frame, sizeof(double) * 10 * njobs, &d_fr)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(tgt_off, sizeof(int64_t) * (njobs + 1), &d_off)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(tgt, sizeof(int) * npairs, &d_tgt)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(xu, sizeof(double) * tab, &d_xu)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(wu, sizeof(double) * tab, &d_wu)) != cudaSuccess) return fail(e, "upload");
+    if ((e = upload(ex, sizeof(double) * tab * nq, &d_ex)) != cudaSuccess) return fail(e, "upload");
+    if ((e = cudaMalloc(&d_out, sizeof(double) * (size_t)npairs * np * np)) != cudaSuccess) return fail(e, "cudaMalloc");
+    bufs.push_back(d_out);
+    const int nu2 = max_up * max_up;
+    const size_t smem = sizeof(double) * (3 * (size_t)nu2 + 2 * (size_t)np * nu2);
+    if (smem > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(k_upsampled_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+        return fail(e, "cudaFuncSetAttribute");
+    k_upsampled_blocks<<<njobs, 256, smem>>>(nq, (const double*)d_pts, (const double*)d_w, (const double*)d_nrm,
+                                             (const int*)d_js, (const int*)d_jn, (const double*)d_fr,
+                                             (const int64_t*)d_off, (const int*)d_tgt, (const double*)d_xu,
+                                             (const double*)d_wu, (const double*)d_ex, (double*)d_out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "k_upsampled_blocks launch");
+    if ((e = cudaMemcpy(out, d_out, sizeof(double) * (size_t)npairs * np * np, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return fail(e, "k_upsampled_blocks");
+    for (void* p : bufs) cudaFree(p);
+    cudaSetDevice(prev);
+    return 0;
+}
 
 int adaptive_blocks_gpu(int device, int nq, int ngl, const double* glx, const double* bary, const double* xg,
                         const double* wg, const double* pts, int64_t npts, const double* normals, int npanels,

@@ -105,8 +105,9 @@ typedef struct {
     int adaptive_n_GL;         /* 0 => n_quad */
     int adaptive_max_depth;    /* default 20 */
     int nthreads;              /* host threads, 0 = all */
-    int device;                /* >= 0: the adaptive (touching-pair) blocks' moment sums run on this CUDA
-                                  device, bitwise equal to the host's (n_quad <= 6); -1 = host only */
+    int device;                /* >= 0: the adaptive (touching-pair) blocks' moment sums and the upsampled
+                                  blocks of sources with n_up <= 8 run on this CUDA device, bitwise equal
+                                  to the host's (n_quad <= 6); -1 = host only */
 } bie_near_opts;
 void bie_near_opts_default(bie_near_opts* o);
 

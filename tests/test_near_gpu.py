@@ -1,6 +1,8 @@
-"""Adaptive (touching-pair) correction blocks computed on the GPU equal the host's
-bitwise: the kernel follows the host's operation order with explicitly rounded
-arithmetic (src/kernel/laplace3d_near_adaptive.jl:308-387 is the reference sum)."""
+"""Correction blocks computed on the GPU equal the host's bitwise: the adaptive
+(touching-pair) moment sums (src/kernel/laplace3d_near_adaptive.jl:308-387) and the
+upsampled blocks (src/kernel/laplace3d_near_upsampling.jl:127-270: Mt K_up - K_direct per
+near pair, one upsampling order per source panel). Both kernels follow the host's
+operation order with explicitly rounded arithmetic."""
 import numpy as np
 import pytest
 
@@ -13,7 +15,7 @@ def test_adaptive_blocks_gpu_bitwise_equal_host(bie, cfg):
     host = itf.near(8, 1e-9, True, setup_device=-1)
     itf2 = bie.single_dielectric_box3d(*cfg)
     dev = itf2.near(8, 1e-9, True, setup_device=0)
-    assert len(dev.adaptive) > 0
+    assert len(dev.adaptive) > 0 and len(dev.upsample) > 0
     assert np.array_equal(host.rowptr, dev.rowptr)
     assert np.array_equal(host.col, dev.col)
     assert np.array_equal(host.val, dev.val)
