@@ -45,7 +45,7 @@ WORKLOADS = {
     # serving stream of uneven geometries (sides U[0.5, 2], eps_in log-U[2, 80], n_quad 4 or 6, node
     # counts log-U[n_min, n_max], geometry repeats with p = 0.5, 1-32 point sources per request)
     "cfg4": dict(requests=2000, n_min=2000, n_max=200000, repeat=0.5, rate=20.0, seed=4, rtol=1e-8,
-                 up_tol=1e-9, max_order=8, k=0, restart=60, resident_fraction=0.5),
+                 up_tol=1e-9, max_order=8, k=0, restart=60, resident_fraction=0.5, builders=4),
 }
 
 # lattice of 4 x 4 x 2 cubes (side 0.5, gap 0.2), 16 sources at cell-corner centres between cubes
@@ -394,12 +394,14 @@ class GeometryCache:
     released) under a device-memory budget. A request's geometry is built when first needed
     (its set-up time falls on that request); least recently used geometries without pending
     requests are destroyed to make room and built again when a later request repeats them.
-    Thread-safe: the submitting thread builds and pins, the polling thread unpins."""
+    Thread-safe: builder threads build and pin (a geometry requested while it is being built
+    waits for that build), the polling thread unpins."""
 
-    def __init__(self, bie, wl, device, budget_bytes):
+    def __init__(self, bie, wl, device, budget_bytes, nthreads=0):
         import collections
-        self.bie, self.wl, self.device, self.budget = bie, wl, device, budget_bytes
+        self.bie, self.wl, self.device, self.budget, self.nthreads = bie, wl, device, budget_bytes, nthreads
         self.live = collections.OrderedDict()  # key -> (itf, op, bytes)
+        self.building = {}                     # key -> Event set when its build ends
         self.lec = {}                          # key -> l_ec found by the first build
         self.pins = collections.Counter()
         self.lock = threading.Lock()
@@ -421,13 +423,31 @@ class GeometryCache:
 
     def get(self, key, spec):
         """(itf, op) of the request's geometry, built if it is not resident; pins it."""
+        while True:
+            with self.lock:
+                if key in self.live:
+                    self.live.move_to_end(key)
+                    self.pins[key] += 1
+                    return self.live[key][:2]
+                ev = self.building.get(key)
+                if ev is None:  # this thread builds it
+                    ev = self.building[key] = threading.Event()
+                    break
+            ev.wait()  # another thread is building it
+        try:
+            return self._build(key, spec)
+        finally:
+            with self.lock:
+                del self.building[key]
+            ev.set()
+
+    def resident(self, key):
+        with self.lock:
+            return key in self.live
+
+    def _build(self, key, spec):
         import ctypes as C
         from dielectricbie_jl_b200 import _abi
-        with self.lock:
-            if key in self.live:
-                self.live.move_to_end(key)
-                self.pins[key] += 1
-                return self.live[key][:2]
         sides, nq, eps_in, target = spec
         t1 = time.perf_counter()
         if key in self.lec:
@@ -438,7 +458,8 @@ class GeometryCache:
             # room for this geometry's blocks (estimated from the first build's size when known)
             self._evict_for(self.live_estimate(itf))
         op = self.bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, self.wl["up_tol"], self.wl["max_order"],
-                                                           device=self.device, keep_host_blocks=False)
+                                                           device=self.device, keep_host_blocks=False,
+                                                           nthreads=self.nthreads)
         n, nb, b = C.c_int64(), C.c_int64(), C.c_size_t()
         _abi.check(_abi.lib().bie_geom_info(op.geom._h, C.byref(n), C.byref(nb), C.byref(b)))
         dt = time.perf_counter() - t1
@@ -496,32 +517,48 @@ def run_serving_workload(args, wl, bie, device):
     total = torch.cuda.get_device_properties(device).total_memory
     budget = int(wl["resident_fraction"] * total)
 
+    builders = wl["builders"]
+
     def run_arm(served):
-        cache = GeometryCache(bie, wl, device, budget)
+        # the served arm builds new geometries on a pool of threads (each with its share of
+        # the host cores), so requests on resident geometries are not held behind set-up; the
+        # plain arm does everything in turn
+        cache = GeometryCache(bie, wl, device, budget,
+                              nthreads=max(2, (os.cpu_count() or 8) // builders) if served else 0)
         nreq = len(reqs)
         lat, done, cols, unsolved = [0.0] * nreq, [0.0] * nreq, 0, 0
         t0 = time.perf_counter() + 0.01
         failed = []
         if served:
             # the server's workspace budget: the device memory the resident geometries leave
-            srv = bie.SolveServer(max_slots=4, max_batch_rhs=128, hbm_fraction=max(0.1, 0.85 - wl["resident_fraction"]))
+            srv = bie.SolveServer(max_slots=4, max_batch_rhs=128, hbm_fraction=max(0.1, 0.7 - wl["resident_fraction"]))
             tickets = [None] * nreq
             sub_t = [0.0] * nreq
             ready = [threading.Event() for _ in range(nreq)]
+
+            def submit_one(i):
+                key, src, a = reqs[i]
+                try:
+                    itf, op = cache.get(key, specs[key])
+                    sub_t[i] = time.perf_counter()
+                    tickets[i] = srv.submit_sources(op, src, specs[key][2], rtol=wl["rtol"],
+                                                    precision=args.precision, restart=wl["restart"])
+                except Exception as e:  # recorded; the stream goes on
+                    failed.append((i, repr(e)))
+                ready[i].set()
+
+            from concurrent.futures import ThreadPoolExecutor
+            pool = ThreadPoolExecutor(max_workers=builders)
 
             def submitter():
                 for i, (key, src, a) in enumerate(reqs):
                     dt = t0 + a - time.perf_counter()
                     if dt > 0:
                         time.sleep(dt)
-                    try:
-                        itf, op = cache.get(key, specs[key])
-                        sub_t[i] = time.perf_counter()
-                        tickets[i] = srv.submit_sources(op, src, specs[key][2], rtol=wl["rtol"],
-                                                        precision=args.precision, restart=wl["restart"])
-                    except Exception as e:  # recorded; the stream goes on
-                        failed.append((i, repr(e)))
-                    ready[i].set()
+                    if cache.resident(key):
+                        submit_one(i)
+                    else:
+                        pool.submit(submit_one, i)
 
             th = threading.Thread(target=submitter)
             th.start()
@@ -537,6 +574,7 @@ def run_serving_workload(args, wl, bie, device):
                 lat[i] = (done[i] - (t0 + reqs[i][2])) * 1e3
                 unsolved += int(not st.solved)
             th.join()
+            pool.shutdown()
             cnt = srv.counters()
             srv.close()
         else:
@@ -594,7 +632,8 @@ def run_serving_workload(args, wl, bie, device):
                        "geometries": len(specs),
                        "geometry_residency": f"built on first use, least recently used idle geometries destroyed "
                                              f"above {wl['resident_fraction']:.0%} of device memory and rebuilt "
-                                             f"when repeated; set-up on the request path of both arms",
+                                             f"when repeated; set-up on the request path of both arms (served: "
+                                             f"{builders} builder threads; plain: in turn)",
                        "host_peak_rss_gb": resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 2**20},
             "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
             "refined_served": served, "plain_fp64_sequential": plain,
@@ -733,6 +772,8 @@ def main():
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--block", type=int, default=0, choices=[0, 1],
+                    help="1: block GMRES (one Krylov space shared by the block's columns)")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-stream measurement")
     ap.add_argument("--profile-matvec", action="store_true",
                     help="apply the refined and the FP64 operator once each to k columns and exit "
@@ -815,6 +856,7 @@ def main():
         o.rtol, o.itmax, o.restart = rtol, 600, 200
         o.precision = _abi.PRECISIONS[precision]
         o.flags = 0 if verify else _abi.BIE_NO_VERIFY
+        o.block = int(args.block)
         return o
 
     def solve_step(i, precision, rtol, verify=False, st=None, allow_noconv=False):
@@ -1050,7 +1092,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"{args.precision} tensor-core direct sum + fp64",
             "data": "synthetic (seeded point sources, uniform in the box interior)",
-            "config": workload_config(args.workload, wl, n),
+            "config": dict(workload_config(args.workload, wl, n),
+                           krylov="block GMRES (one Krylov space per block)" if args.block
+                           else "GMRES, one Arnoldi process per column"),
             "p50_ms": float(np.percentile(ms_ref, 50)), "p99_ms": float(np.percentile(ms_ref, 99)),
             "plain_fp64": {"value": plain_value, "unit": "solves/s", "ms_per_step": total_plain / args.steps,
                            "p50_ms": float(np.percentile(ms_plain, 50)),

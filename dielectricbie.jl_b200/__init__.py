@@ -424,12 +424,13 @@ class GPUDielectricOperator:
 
     def __init__(self, interface: DielectricInterface, *, precision: str = "fp64", corrections: bool = True,
                  up_tol: float = 1e-9, max_order: int = 8, correct_edges: bool = True,
-                 adaptive_cfg: Optional[AdaptiveConfig] = None, device: int = 0, keep_host_blocks: bool = True):
+                 adaptive_cfg: Optional[AdaptiveConfig] = None, device: int = 0, keep_host_blocks: bool = True,
+                 nthreads: int = 0):
         if precision not in _abi.PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_abi.PRECISIONS)}")
         self.interface = interface
         self.precision = precision
-        self.near = interface.near(max_order, up_tol, correct_edges, adaptive_cfg) if corrections else None
+        self.near = interface.near(max_order, up_tol, correct_edges, adaptive_cfg, nthreads) if corrections else None
         self.geom = interface.geom(self.near, device)
         if self.near is not None and not keep_host_blocks:
             # the blocks live on the device only (a server's many resident geometries)
@@ -489,15 +490,17 @@ def lhs_dielectric_box3d_fmm3d_corrected(interface: DielectricInterface, fmm_tol
                                          max_order: int, *, correct_edges: bool = True,
                                          adaptive_atol: Optional[float] = None, adaptive_rtol: float = SQRT_EPS,
                                          adaptive_n_GL: int = 0, adaptive_max_depth: int = 20,
-                                         precision: str = "fp64", device: int = 0, keep_host_blocks: bool = True):
+                                         precision: str = "fp64", device: int = 0, keep_host_blocks: bool = True,
+                                         nthreads: int = 0):
     """``lhs_dielectric_box3d_fmm3d_corrected`` (src/solver/dielectric_box3d.jl:48-92).
     keep_host_blocks=False frees the host copy of the correction blocks once they are on the
-    device (they are read back from there on request)."""
+    device (they are read back from there on request); nthreads bounds the host threads of
+    the near-field set-up (0 = all)."""
     ad = AdaptiveConfig(up_tol if adaptive_atol is None else adaptive_atol, adaptive_rtol, adaptive_n_GL,
                         adaptive_max_depth)
     return GPUDielectricOperator(interface, precision=precision, corrections=True, up_tol=up_tol,
                                  max_order=max_order, correct_edges=correct_edges, adaptive_cfg=ad, device=device,
-                                 keep_host_blocks=keep_host_blocks)
+                                 keep_host_blocks=keep_host_blocks, nthreads=nthreads)
 
 
 def batched_lhs_dielectric_box3d_fmm3d_corrected(interface, fmm_tol, up_tol, max_order, **kw):
@@ -669,12 +672,14 @@ class SolveStats:
     col_resid: np.ndarray
 
 
-def _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every):
+def _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every,
+                block=False):
     o = _abi.SolveOpts()
     lib().bie_solve_opts_default(C.byref(o))
     o.atol, o.rtol, o.itmax, o.restart = float(atol), float(rtol), int(itmax), int(restart)
     o.precision = _abi.PRECISIONS[precision or op.precision]
     o.inner_rtol, o.max_outer, o.precondition, o.check_every = float(inner_rtol), int(max_outer), int(precondition), int(check_every)
+    o.block = int(bool(block))
     if op.near is None:
         o.flags = 0
     return o
@@ -682,11 +687,13 @@ def _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer
 
 def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float = 0.0, itmax: int = 500,
               restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
-              precondition: bool = False, check_every: int = 1, raise_on_noconv: bool = False):
-    """Solve A Sigma = F on the device. Returns (Sigma, SolveStats)."""
+              precondition: bool = False, check_every: int = 1, raise_on_noconv: bool = False, block: bool = False):
+    """Solve A Sigma = F on the device. Returns (Sigma, SolveStats). block=True runs block GMRES
+    (one Krylov space shared by the columns, as Krylov.block_gmres) for more than one column."""
     Ff, vec = _as_cols(F, op.n)
     k = Ff.shape[1]
-    o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+    o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every,
+                    block)
     S, stats = _run_solve(op, k, raise_on_noconv,
                           lambda S, st: lib().bie_solve(op.geom._h, dptr(Ff), dptr(S), k, C.byref(o), C.byref(st)))
     return (S[:, 0] if vec else S), stats
@@ -710,13 +717,14 @@ def _run_solve(op, k, raise_on_noconv, call):
 def gpu_solve_sources(op: GPUDielectricOperator, sources, eps_src, *, rtol: float = 1e-10, atol: float = 0.0,
                       itmax: int = 500, restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6,
                       max_outer: int = 8, precondition: bool = False, check_every: int = 1,
-                      raise_on_noconv: bool = False):
+                      raise_on_noconv: bool = False, block: bool = False):
     """rhs_dielectric_box3d for point sources and the block solve in one call (C-ABI
     ``bie_solve_point``): the right-hand sides are built on the device, so only the sources
     go to the GPU and only Sigma comes back. Returns (Sigma N x k, SolveStats)."""
     src, q, eps = _point_sources(sources, eps_src)
     k = len(q)
-    o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+    o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every,
+                    block)
     return _run_solve(op, k, raise_on_noconv,
                       lambda S, st: lib().bie_solve_point(op.geom._h, dptr(src), dptr(q), dptr(eps), k, dptr(S),
                                                           C.byref(o), C.byref(st)))
@@ -764,10 +772,11 @@ class SolveServer:
 
     def submit(self, op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float = 0.0, itmax: int = 500,
                restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
-               precondition: bool = False, check_every: int = 1) -> int:
+               precondition: bool = False, check_every: int = 1, block: bool = False) -> int:
         Ff, vec = _as_cols(F, op.n)
         k = Ff.shape[1]
-        o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+        o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every,
+                    block)
         t = C.c_uint64(0)
         check(lib().bie_server_submit(self._h, op.geom._h, dptr(Ff), k, C.byref(o), C.byref(t)))
         self._shapes[t.value] = (op.n, k, vec)
@@ -776,13 +785,14 @@ class SolveServer:
     def submit_sources(self, op: GPUDielectricOperator, sources, eps_src, *, rtol: float = 1e-10, atol: float = 0.0,
                        itmax: int = 500, restart: int = 200, precision: Optional[str] = None,
                        inner_rtol: float = 1e-6, max_outer: int = 8, precondition: bool = False,
-                       check_every: int = 1) -> int:
+                       check_every: int = 1, block: bool = False) -> int:
         """Queues the block solve of point-source right-hand sides (C-ABI
         ``bie_server_submit_point``): only the sources are held until the batch runs, which
         builds the right-hand sides on the device. The result is N x k as for submit()."""
         src, q, eps = _point_sources(sources, eps_src)
         k = len(q)
-        o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every)
+        o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every,
+                    block)
         t = C.c_uint64(0)
         check(lib().bie_server_submit_point(self._h, op.geom._h, dptr(src), dptr(q), dptr(eps), k, C.byref(o),
                                             C.byref(t)))

@@ -54,7 +54,7 @@ class NearOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("atol", C.c_double), ("rtol", C.c_double), ("itmax", C.c_int), ("restart", C.c_int),
                 ("precision", C.c_int), ("inner_rtol", C.c_double), ("max_outer", C.c_int),
-                ("precondition", C.c_int), ("check_every", C.c_int), ("flags", C.c_uint32)]
+                ("precondition", C.c_int), ("check_every", C.c_int), ("flags", C.c_uint32), ("block", C.c_int)]
 
 
 class ServerOpts(C.Structure):

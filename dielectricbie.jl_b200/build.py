@@ -3,7 +3,8 @@
     python dielectricbie.jl_b200/build.py [--force]
 
 The shared library lands next to this file so that it travels with the source
-tree; CUDA runtime is linked statically (only libcuda.so is needed at run time).
+tree; CUDA runtime is linked statically (libcuda.so and the toolkit's libcublas.so, found
+through the rpath, are needed at run time).
 """
 from __future__ import annotations
 
@@ -75,7 +76,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
                        check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    subprocess.run([nvcc, "-ccbin", cxx, *ARCH, "-shared", "-o", tmp, *objs, "-Xcompiler", "-fopenmp", "-lgomp"],
+    # cuBLAS (the block GMRES basis products) from the CUDA toolkit, found through the rpath
+    cudalib = os.path.join(os.path.dirname(os.path.dirname(nvcc)), "lib64")
+    subprocess.run([nvcc, "-ccbin", cxx, *ARCH, "-shared", "-o", tmp, *objs, "-Xcompiler", "-fopenmp", "-lgomp",
+                    "-L", cudalib, "-lcublas", "-Xlinker", "-rpath," + cudalib, "-Xlinker", "--no-undefined"],
                    check=True)
     os.replace(tmp, LIB)
     return LIB

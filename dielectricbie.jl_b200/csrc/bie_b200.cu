@@ -600,6 +600,7 @@ void bie_solve_opts_default(bie_solve_opts* o) {
     o->precondition = 0;
     o->check_every = 1;
     o->flags = 0;
+    o->block = 0;
 }
 
 int bie_solve(bie_geom* g, const double* F, double* Sigma, int32_t k, const bie_solve_opts* o, bie_stats* st) {

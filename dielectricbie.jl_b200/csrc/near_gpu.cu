@@ -235,8 +235,16 @@ int upsampled_blocks_gpu(int device, int nq, const double* pts, int64_t npts, co
     int prev = 0;
     cudaGetDevice(&prev);
     std::vector<void*> bufs;
+    // set-up work runs on its own non-blocking stream with stream-ordered allocations, so it
+    // neither waits for nor stalls the solves running on other streams (a cudaFree would
+    // synchronise the whole device)
+    cudaStream_t st = nullptr;
     auto fail = [&](cudaError_t e, const char* what) {
-        for (void* p : bufs) cudaFree(p);
+        for (void* p : bufs) cudaFreeAsync(p, st);
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
         cudaSetDevice(prev);
         err = std::string(what) + ": " + cudaGetErrorString(e);
         cudaGetLastError();
@@ -244,11 +252,18 @@ int upsampled_blocks_gpu(int device, int nq, const double* pts, int64_t npts, co
     };
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
     auto upload = [&](const void* src, size_t bytes, void** dst) -> cudaError_t {
-        cudaError_t r = cudaMalloc(dst, bytes > 0 ? bytes : 8);
+        cudaError_t r = cudaMallocAsync(dst, bytes > 0 ? bytes : 8, st);
         if (r != cudaSuccess) return r;
         bufs.push_back(*dst);
-        return bytes ? cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+        return bytes ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+    };
+    auto finish = [&]() {
+        for (void* p : bufs) cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        cudaSetDevice(prev);
     };
     const size_t tab = (size_t)(kMaxUp + 1) * (kMaxUp + 1);
     void *d_pts, *d_w, *d_nrm, *d_js, *d_jn, *d_fr, *d_off, *d_tgt, *d_xu, *d_wu, *d_ex, *d_out;
@@ -263,7 +278,8 @@ int upsampled_blocks_gpu(int device, int nq, const double* pts, int64_t npts, co
     if ((e = upload(xu, sizeof(double) * tab, &d_xu)) != cudaSuccess) return fail(e, "upload");
     if ((e = upload(wu, sizeof(double) * tab, &d_wu)) != cudaSuccess) return fail(e, "upload");
     if ((e = upload(ex, sizeof(double) * tab * nq, &d_ex)) != cudaSuccess) return fail(e, "upload");
-    if ((e = cudaMalloc(&d_out, sizeof(double) * (size_t)npairs * np * np)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMallocAsync(&d_out, sizeof(double) * (size_t)npairs * np * np, st)) != cudaSuccess)
+        return fail(e, "cudaMallocAsync");
     bufs.push_back(d_out);
     const int nu2 = max_up * max_up;
     const size_t smem = sizeof(double) * (3 * (size_t)nu2 + 2 * (size_t)np * nu2);
@@ -271,15 +287,16 @@ int upsampled_blocks_gpu(int device, int nq, const double* pts, int64_t npts, co
         (e = cudaFuncSetAttribute(k_upsampled_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
-    k_upsampled_blocks<<<njobs, 256, smem>>>(nq, (const double*)d_pts, (const double*)d_w, (const double*)d_nrm,
+    k_upsampled_blocks<<<njobs, 256, smem, st>>>(nq, (const double*)d_pts, (const double*)d_w, (const double*)d_nrm,
                                              (const int*)d_js, (const int*)d_jn, (const double*)d_fr,
                                              (const int64_t*)d_off, (const int*)d_tgt, (const double*)d_xu,
                                              (const double*)d_wu, (const double*)d_ex, (double*)d_out);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "k_upsampled_blocks launch");
-    if ((e = cudaMemcpy(out, d_out, sizeof(double) * (size_t)npairs * np * np, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)npairs * np * np, cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return fail(e, "k_upsampled_blocks");
-    for (void* p : bufs) cudaFree(p);
-    cudaSetDevice(prev);
+    finish();
     return 0;
 }
 
@@ -308,8 +325,16 @@ int adaptive_blocks_gpu(int device, int nq, int ngl, const double* glx, const do
     int prev = 0;
     cudaGetDevice(&prev);
     std::vector<void*> bufs;
+    // set-up work runs on its own non-blocking stream with stream-ordered allocations, so it
+    // neither waits for nor stalls the solves running on other streams (a cudaFree would
+    // synchronise the whole device)
+    cudaStream_t st = nullptr;
     auto fail = [&](cudaError_t e, const char* what) {
-        for (void* p : bufs) cudaFree(p);
+        for (void* p : bufs) cudaFreeAsync(p, st);
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
         cudaSetDevice(prev);
         err = std::string(what) + ": " + cudaGetErrorString(e);
         cudaGetLastError();
@@ -317,11 +342,18 @@ int adaptive_blocks_gpu(int device, int nq, int ngl, const double* glx, const do
     };
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
     auto upload = [&](const void* src, size_t bytes, void** dst) -> cudaError_t {
-        cudaError_t r = cudaMalloc(dst, bytes > 0 ? bytes : 8);
+        cudaError_t r = cudaMallocAsync(dst, bytes > 0 ? bytes : 8, st);
         if (r != cudaSuccess) return r;
         bufs.push_back(*dst);
-        return bytes ? cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+        return bytes ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+    };
+    auto finish = [&]() {
+        for (void* p : bufs) cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        cudaSetDevice(prev);
     };
     void *d_pts, *d_nrm, *d_fr, *d_trg, *d_off, *d_leaves, *d_kb;
     if ((e = upload(pts, sizeof(double) * 3 * npts, &d_pts)) != cudaSuccess) return fail(e, "upload");
@@ -330,21 +362,23 @@ int adaptive_blocks_gpu(int device, int nq, int ngl, const double* glx, const do
     if ((e = upload(trg, sizeof(int) * npairs, &d_trg)) != cudaSuccess) return fail(e, "upload");
     if ((e = upload(leaf_off, sizeof(int64_t) * (npairs + 1), &d_off)) != cudaSuccess) return fail(e, "upload");
     if ((e = upload(leaves, sizeof(double) * 4 * nleaves, &d_leaves)) != cudaSuccess) return fail(e, "upload");
-    if ((e = cudaMalloc(&d_kb, sizeof(double) * (size_t)npairs * np * np)) != cudaSuccess) return fail(e, "cudaMalloc");
+    if ((e = cudaMallocAsync(&d_kb, sizeof(double) * (size_t)npairs * np * np, st)) != cudaSuccess)
+        return fail(e, "cudaMallocAsync");
     bufs.push_back(d_kb);
     const size_t smem = sizeof(double) * ((size_t)ngl * ngl * np + 2 * ngl * nq + ngl * ngl);
     if (smem > 48 * 1024 &&
         (e = cudaFuncSetAttribute(k_adaptive_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
             cudaSuccess)
         return fail(e, "cudaFuncSetAttribute");
-    k_adaptive_blocks<<<npairs, 256, smem>>>(tb, (const double*)d_pts, (const double*)d_nrm, (const double*)d_fr,
+    k_adaptive_blocks<<<npairs, 256, smem, st>>>(tb, (const double*)d_pts, (const double*)d_nrm, (const double*)d_fr,
                                              (const int*)d_trg, (const int64_t*)d_off, (const double*)d_leaves,
                                              (double*)d_kb);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "k_adaptive_blocks launch");
-    if ((e = cudaMemcpy(Kb, d_kb, sizeof(double) * (size_t)npairs * np * np, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(Kb, d_kb, sizeof(double) * (size_t)npairs * np * np, cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return fail(e, "k_adaptive_blocks");
-    for (void* p : bufs) cudaFree(p);
-    cudaSetDevice(prev);
+    finish();
     return 0;
 }
 

@@ -66,7 +66,8 @@ struct Request {
 bool same_opts(const bie_solve_opts& a, const bie_solve_opts& b) {
     return a.atol == b.atol && a.rtol == b.rtol && a.itmax == b.itmax && a.restart == b.restart &&
            a.precision == b.precision && a.inner_rtol == b.inner_rtol && a.max_outer == b.max_outer &&
-           a.precondition == b.precondition && a.check_every == b.check_every && a.flags == b.flags;
+           a.precondition == b.precondition && a.check_every == b.check_every && a.flags == b.flags &&
+           a.block == b.block;
 }
 
 // Device workspace of a block solve of k columns: the Krylov basis (restart + 1

@@ -1,5 +1,6 @@
 // Device-resident geometry, layer-potential operators and the device GMRES /
 // iterative-refinement solvers of libbie_b200.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -16,6 +17,7 @@
 #include <utility>
 #include <vector>
 
+#include "bgmres.cuh"
 #include "kernels.cuh"
 #include "solver.h"
 
@@ -34,6 +36,9 @@ struct bie_geom {
     int max_row_blocks = 0;  // longest BSR block row (blocks of one target panel)
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
+    // block GMRES workspace: basis, Hessenberg matrix, right-hand sides, small factors
+    bie::Buf bv, bq, bvj, bh, bgv, btau, br1, br2, br, bh2, bres, bidx, bflag, xa, ra, binv, bpart, btmp;
+    cublasHandle_t blas = nullptr;  // created on the first block solve
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // kernel timing
     struct ProfRec {
@@ -699,7 +704,7 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
         // residual of the current cycle
         const double* r = dr;
         if (!first) {
-            apply_op(g, dx, W, k, prec, flags, pre, s);
+            apply_op(g, dx, W, k, prec, flags, nullptr, s);  // dx holds x = p .* u: the true residual
             ++res.matvecs;
             BIE_CK(cudaMemcpyAsync(g->rr.p, dr, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
             {
@@ -824,6 +829,245 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
     }
     if (signature() == gc->sig) gc->warm = true;
     res.iters = it;
+    return res;
+}
+
+// ------------------------------ block GMRES ----------------------------------
+void blas_ck(cublasStatus_t st, const char* what) {
+    if (st != CUBLAS_STATUS_SUCCESS)
+        throw Error(st == CUBLAS_STATUS_ALLOC_FAILED ? BIE_ENOMEM : BIE_ECUDA,
+                    std::string("cuBLAS ") + what + " failed (status " + std::to_string((int)st) + ")");
+}
+
+cublasHandle_t blas_handle(bie_geom* g, cudaStream_t s) {
+    if (!g->blas) blas_ck(cublasCreate(&g->blas), "create");
+    blas_ck(cublasSetStream(g->blas, s), "set stream");
+    return g->blas;
+}
+
+// G (ka x ka, ld ka) = Q Q^T for Q ka x n (ld ka): partial Gram matrices of up to 148 column
+// chunks (one batched DGEMM, a second for the remainder), summed in a fixed order.
+void gram(bie_geom* g, cublasHandle_t h, const double* Q, int ka, int64_t n, double* G, cudaStream_t s) {
+    const double one = 1.0, zero = 0.0;
+    const int64_t nb_want = std::max<int64_t>(1, std::min<int64_t>(148, n / 256));
+    const int64_t c = (n + nb_want - 1) / nb_want;
+    const int64_t nfull = n / c, rem = n - nfull * c;
+    const int nb = (int)(nfull + (rem > 0 ? 1 : 0));
+    const int64_t kk = (int64_t)ka * ka;
+    g->bpart.ensure(sizeof(double) * (size_t)nb * kk);
+    double* P = g->bpart.as<double>();
+    if (nfull > 0)
+        blas_ck(cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, ka, ka, (int)c, &one, Q, ka, c * ka, Q, ka,
+                                          c * ka, &zero, P, ka, kk, (int)nfull),
+                "gemm (batched)");
+    if (rem > 0)
+        blas_ck(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, ka, ka, (int)rem, &one, Q + nfull * c * ka, ka,
+                            Q + nfull * c * ka, ka, &zero, P + nfull * kk, ka),
+                "gemm");
+    k_sum_partials<<<grid1(kk), 256, 0, s>>>(P, nb, (int)kk, G);
+    BIE_CK(cudaGetLastError());
+}
+
+// Orthonormalises the rows of Q (ka x n, column-major, ld ka: the transposed block of ka
+// vectors) by Cholesky QR applied twice: Q_old = R^T Q_new, R = R2 R1 (ka x ka upper) into
+// Rout (ld ldr). Up to 64 columns the Gram matrix comes from chunked DGEMMs, is factored and
+// inverted in shared memory and applied as a DGEMM with R^-T; wider blocks use SYRK and TRSM.
+void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double* Rout, int ldr, cudaStream_t s) {
+    const double one = 1.0, zero = 0.0;
+    double* R1 = g->br1.as<double>();
+    double* R2 = g->br2.as<double>();
+    if (ka <= 64) {
+        g->binv.ensure(sizeof(double) * (size_t)ka * ka);
+        g->btmp.ensure(sizeof(double) * (size_t)n * ka);
+        double* Gm = g->br.as<double>();
+        double* Ri = g->binv.as<double>();
+        double* tmp = g->btmp.as<double>();
+        const size_t sm = 2 * sizeof(double) * (size_t)ka * ka;
+        ensure_smem_limit((const void*)k_chol_inv_smem, sm);
+        for (int pass = 0; pass < 2; ++pass) {
+            double* Rp = pass == 0 ? R1 : R2;
+            gram(g, h, Q, ka, n, Gm, s);
+            k_chol_inv_smem<<<1, 256, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
+            BIE_CK(cudaGetLastError());
+            blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, ka, &one, Ri, ka, Q, ka, &zero, tmp, ka),
+                    "gemm");
+            BIE_CK(cudaMemcpyAsync(Q, tmp, sizeof(double) * (size_t)n * ka, cudaMemcpyDeviceToDevice, s));
+        }
+    } else {
+        for (int pass = 0; pass < 2; ++pass) {
+            double* Rp = pass == 0 ? R1 : R2;
+            blas_ck(cublasDsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, ka, (int)n, &one, Q, ka, &zero, Rp, ka),
+                    "syrk");
+            k_chol_upper<<<1, 256, 0, s>>>(Rp, ka, ka, g->bflag.as<int>());
+            BIE_CK(cudaGetLastError());
+            blas_ck(cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, ka,
+                                (int)n, &one, Rp, ka, Q, ka),
+                    "trsm");
+        }
+    }
+    k_trmm_upper<<<grid1((int64_t)ka * ka), 256, 0, s>>>(R2, ka, R1, ka, Rout, ldr, ka);
+    BIE_CK(cudaGetLastError());
+}
+
+// Block GMRES (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285): the active
+// columns of dr share one block Krylov space. Block Arnoldi with classical Gram-Schmidt
+// against the whole basis (two passes for FP64 solves, one for the reduced-precision inner
+// solves), each new block orthonormalised by Cholesky QR applied twice; the block
+// upper-Hessenberg least-squares problem is updated by Householder reflections one block
+// column per iteration, which gives every column's residual norm. The tall-skinny products
+// with the basis are cuBLAS DGEMMs. The basis is kept as the rows of M ((m + 1) ka x n,
+// column-major: node i holds all basis values in a row of M's column i). Solves
+// A(p .* u) = r, x = p .* u into dx (node-major n x k, zero in the inactive columns);
+// m = block iterations per cycle (restart, at most 60).
+GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
+                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, cudaStream_t s) {
+    const int64_t n = g->n;
+    const bool one_pass = prec != BIE_FP64;
+    GmresResult res;
+    res.col_iters.assign(k, 0);
+    BIE_CK(cudaMemsetAsync(dx, 0, sizeof(double) * n * k, s));
+    // columns that need work: active and above their tolerance
+    g->beta.ensure(sizeof(double) * k);
+    col_norms(g, dr, k, g->beta.as<double>(), s);
+    std::vector<double> nr(k);
+    d2h(nr.data(), g->beta.p, k, s);
+    std::vector<int> idx;
+    for (int c = 0; c < k; ++c)
+        if (active0[c] && nr[c] > eps[c]) idx.push_back(c);
+    const int ka = (int)idx.size();
+    if (ka == 0) {
+        res.all_converged = true;
+        return res;
+    }
+    m = std::max(1, std::min({m, itmax, 60}));
+    const int64_t L = (int64_t)(m + 1) * ka;  // rows of the basis and of the Hessenberg matrix
+    const int64_t nka = n * ka;
+    g->bv.ensure(sizeof(double) * (size_t)L * n);
+    g->bq.ensure(sizeof(double) * nka);
+    g->bvj.ensure(sizeof(double) * nka);
+    g->bh.ensure(sizeof(double) * (size_t)L * m * ka);
+    g->bgv.ensure(sizeof(double) * (size_t)L * ka);
+    g->btau.ensure(sizeof(double) * (size_t)m * ka);
+    g->br1.ensure(sizeof(double) * (size_t)ka * ka);
+    g->br2.ensure(sizeof(double) * (size_t)ka * ka);
+    g->br.ensure(sizeof(double) * (size_t)ka * ka);
+    g->bh2.ensure(sizeof(double) * (size_t)L * ka);
+    g->bres.ensure(sizeof(double) * ka);
+    g->bidx.ensure(sizeof(int) * ka);
+    g->bflag.ensure(sizeof(int));
+    g->xa.ensure(sizeof(double) * nka);
+    g->ra.ensure(sizeof(double) * nka);
+    upload(g->bidx, idx.data(), ka, s);
+    BIE_CK(cudaMemsetAsync(g->bflag.p, 0, sizeof(int), s));
+    double* M = g->bv.as<double>();
+    double* Q = g->bq.as<double>();
+    double* Vj = g->bvj.as<double>();
+    double* H = g->bh.as<double>();
+    double* Gv = g->bgv.as<double>();
+    double* Xa = g->xa.as<double>();
+    double* Ra = g->ra.as<double>();
+    BIE_CK(cudaMemsetAsync(Xa, 0, sizeof(double) * nka, s));
+    std::vector<double> epsa(ka), rsd(ka);
+    for (int a = 0; a < ka; ++a) epsa[a] = eps[idx[a]];
+    const double one = 1.0, zero = 0.0, mone = -1.0;
+    const size_t pitchL = sizeof(double) * (size_t)L, pitchK = sizeof(double) * (size_t)ka;
+    int it = 0;
+    bool first = true, conv = false;
+    while (true) {
+        // residual of the cycle: the right-hand side, or the true residual of the iterate
+        k_gather_cols<<<grid1(nka), 256, 0, s>>>(dr, k, g->bidx.as<int>(), ka, n, Ra);
+        BIE_CK(cudaGetLastError());
+        if (!first) {
+            apply_op(g, Xa, Q, ka, prec, flags, nullptr, s);
+            ++res.matvecs;
+            k_axpby<<<grid1(nka), 256, 0, s>>>(-1.0, Q, 1.0, Ra, n, ka, nullptr);
+            BIE_CK(cudaGetLastError());
+        }
+        cublasHandle_t h = blas_handle(g, s);
+        BIE_CK(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)L * m * ka, s));
+        BIE_CK(cudaMemsetAsync(Gv, 0, sizeof(double) * (size_t)L * ka, s));
+        // V_0 S_0 = R (Cholesky QR); Gv = [S_0; 0]
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            cholqr2(g, h, Ra, ka, n, Gv, (int)L, s);
+            BIE_CK(cudaMemcpy2DAsync(M, pitchL, Ra, pitchK, pitchK, (size_t)n, cudaMemcpyDeviceToDevice, s));
+        }
+        int jend = 0;
+        for (int j = 0; j < m && it < itmax; ++j) {
+            const int64_t rows = (int64_t)(j + 1) * ka;  // basis vectors so far
+            BIE_CK(cudaMemcpy2DAsync(Vj, pitchK, M + (size_t)j * ka, pitchL, pitchK, (size_t)n,
+                                     cudaMemcpyDeviceToDevice, s));
+            apply_op(g, Vj, Q, ka, prec, flags, pre, s);  // W = A (p .* V_j), held as Q = W^T
+            ++res.matvecs;
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                double* Hc = H + (size_t)j * ka * L;  // block column j
+                // classical Gram-Schmidt: H = V^T W and W -= V H, i.e. H = M_j Q^T, Q -= H^T M_j
+                blas_ck(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)rows, ka, (int)n, &one, M, (int)L, Q, ka, &zero,
+                                    Hc, (int)L),
+                        "gemm");
+                blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, (int)rows, &mone, Hc, (int)L, M, (int)L,
+                                    &one, Q, ka),
+                        "gemm");
+                if (!one_pass) {
+                    double* H2 = g->bh2.as<double>();
+                    blas_ck(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)rows, ka, (int)n, &one, M, (int)L, Q, ka,
+                                        &zero, H2, (int)rows),
+                            "gemm");
+                    blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, (int)rows, &mone, H2, (int)rows, M,
+                                        (int)L, &one, Q, ka),
+                            "gemm");
+                    blas_ck(cublasDgeam(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)rows, ka, &one, Hc, (int)L, &one, H2,
+                                        (int)rows, Hc, (int)L),
+                            "geam");
+                }
+                // the new block: W = V_{j+1} R, R into H's block (j + 1, j)
+                cholqr2(g, h, Q, ka, n, Hc + rows, (int)L, s);
+                BIE_CK(cudaMemcpy2DAsync(M + (size_t)(j + 1) * ka, pitchL, Q, pitchK, pitchK, (size_t)n,
+                                         cudaMemcpyDeviceToDevice, s));
+                // least squares: the Householder QR of block column j and every column's residual
+                if (ka <= 64) {
+                    const size_t sm = sizeof(double) * (4 * (size_t)ka * ka + ka);
+                    ensure_smem_limit((const void*)k_bhess_qr_step_smem, sm);
+                    k_bhess_qr_step_smem<<<1, 256, sm, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
+                                                            g->bres.as<double>());
+                } else {
+                    k_bhess_qr_step<<<1, 256, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
+                                                      g->bres.as<double>());
+                }
+                BIE_CK(cudaGetLastError());
+            }
+            ++it;
+            jend = j + 1;
+            d2h(rsd.data(), g->bres.p, ka, s);
+            bool all = true;
+            for (int a = 0; a < ka; ++a) all = all && rsd[a] <= epsa[a];
+            if (all) {
+                conv = true;
+                break;
+            }
+        }
+        // Y = R^-1 Gv[0 : jend ka], x += p .* (V Y)
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            const int rows = jend * ka;
+            blas_ck(cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, ka,
+                                &one, H, (int)L, Gv, (int)L),
+                    "trsm");
+            blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, rows, &one, Gv, (int)L, M, (int)L, &zero, Q,
+                                ka),
+                    "gemm");
+            k_add_rows_scaled<<<grid1(nka), 256, 0, s>>>(Xa, Q, pre, n, ka);
+            BIE_CK(cudaGetLastError());
+        }
+        if (conv || it >= itmax) break;
+        first = false;
+    }
+    k_scatter_cols<<<grid1(nka), 256, 0, s>>>(Xa, ka, g->bidx.as<int>(), k, n, dx);
+    BIE_CK(cudaGetLastError());
+    for (int a = 0; a < ka; ++a) res.col_iters[idx[a]] = it;
+    res.iters = it;
+    res.all_converged = conv;
     return res;
 }
 
@@ -954,7 +1198,9 @@ void geom_trim(bie_geom* g) {
     BIE_CK(cudaStreamSynchronize(g->stream));
     bie::Buf* ws[] = {&g->part, &g->bpack, &g->cpart, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn, &g->h, &g->h2,
                       &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid, &g->dpart, &g->rr,
-                      &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
+                      &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol, &g->srcpack, &g->glist, &g->bv, &g->bq,
+                      &g->bvj, &g->bh, &g->bgv, &g->btau, &g->br1, &g->br2, &g->br, &g->bh2, &g->bres, &g->bidx,
+                      &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp};
     for (auto* b : ws) b->release();
     for (auto& c : g->gcache) {
         for (auto ex : c.exec)
@@ -1008,8 +1254,11 @@ void geom_destroy(bie_geom* g) {
         bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->perm, &g->rowptr,
                            &g->col, &g->val, &g->part, &g->small, &g->bpack, &g->errflag, &g->cpart, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
-                           &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol};
+                           &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol, &g->srcpack, &g->glist,
+                           &g->bv, &g->bq, &g->bvj, &g->bh, &g->bgv, &g->btau, &g->br1, &g->br2, &g->br, &g->bh2,
+                           &g->bres, &g->bidx, &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp};
         for (auto* b : all) b->release();
+        if (g->blas) cublasDestroy(g->blas);
         for (auto& r : g->prof_pending) {
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
@@ -1207,7 +1456,9 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
     g->xo.ensure(sizeof(double) * nk);
     double* rbuf = g->xo.as<double>();  // outer residual F - A x
     if (o.precision == BIE_FP64) {
-        GmresResult r = gmres(g, dF, dX, k, BIE_FP64, o.flags, pre, tol, act, o.itmax, o.restart, o.check_every, s);
+        GmresResult r = (o.block && k > 1)
+                            ? bgmres(g, dF, dX, k, BIE_FP64, o.flags, pre, tol, act, o.itmax, o.restart, s)
+                            : gmres(g, dF, dX, k, BIE_FP64, o.flags, pre, tol, act, o.itmax, o.restart, o.check_every, s);
         iters = r.iters;
         outer = 1;
         f64mv = r.matvecs;
@@ -1265,7 +1516,10 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             // cannot lower the true residual of this pass)
             for (int c = 0; c < k; ++c)
                 eps_in[c] = std::max({o.inner_rtol * rn[c], 0.5 * tol[c], 2.0 * inner_delta * rn[c]});
-            GmresResult r = gmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
+            GmresResult r = (o.block && k > 1)
+                                ? bgmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
+                                         o.itmax - iters, o.restart, s)
+                                : gmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
                                   o.itmax - iters, o.restart, o.check_every, s);
             iters += r.iters;
             lpmv += r.matvecs;
