@@ -9,7 +9,14 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "kernels.cuh"
+
 namespace bie {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
 
 // In-place Cholesky factor of the symmetric positive (semi)definite k x k matrix G
 // (upper triangle read): G = R^T R with R upper triangular written to the upper triangle,
@@ -55,65 +62,74 @@ __global__ void k_chol_upper(double* __restrict__ G, int k, int ldg, int* __rest
 }
 
 // Cholesky factor R of the k x k Gram matrix G (ld k, upper triangle read) and its inverse,
-// in shared memory (2 k^2 doubles, k <= 64): R into Rout (ld ldr, lower triangle zeroed),
-// R^-1 into Rinv (ld k). Pivots are clamped as in k_chol_upper.
-__global__ void k_chol_inv_smem(const double* __restrict__ G, int k, double* __restrict__ Rout, int ldr,
-                                double* __restrict__ Rinv, int* __restrict__ nclamp) {
+// in shared memory (2 k (k + 1) doubles, k <= 64): R into Rout (ld ldr, lower triangle zeroed),
+// R^-1 into Rinv (ld k). Pivots are clamped as in k_chol_upper. The factorisation is
+// right-looking with one barrier per pivot (row p of the factor goes to its own array while
+// the trailing matrix is updated from the unscaled row); the inverse is formed column by
+// column, one warp per column, by back substitution with the column in registers.
+__global__ void __launch_bounds__(1024) k_chol_inv_smem(const double* __restrict__ G, int k, double* __restrict__ Rout,
+                                                        int ldr, double* __restrict__ Rinv, int* __restrict__ nclamp) {
     extern __shared__ double sm[];
-    double* A = sm;          // k x k
-    double* B = sm + k * k;  // k x k, the inverse
+    const int ld = k + 1;     // padded: a row of the matrix spreads over the shared-memory banks
+    double* A = sm;           // k x k, ld: the trailing matrix
+    double* R = sm + ld * k;  // k x k, ld: the factor
     __shared__ double s_floor;
-    const int tid = threadIdx.x;
+    __shared__ double s_rinv[64];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
     for (int e = tid; e < k * k; e += blockDim.x) {
         const int i = e % k, jj = e / k;
-        A[e] = i <= jj ? G[i + jj * k] : 0.0;
+        A[i + jj * ld] = i <= jj ? G[i + jj * k] : 0.0;
+        R[i + jj * ld] = 0.0;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (warp == 0) {
         double mx = 0.0;
-        for (int i = 0; i < k; ++i) mx = fmax(mx, A[i + i * k]);
-        s_floor = mx > 0.0 ? 1e-30 * mx : 1e-300;
+        for (int i = lane; i < k; i += 32) mx = fmax(mx, A[i + i * ld]);
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        if (lane == 0) s_floor = mx > 0.0 ? 1e-30 * mx : 1e-300;
     }
     __syncthreads();
+    const double fl = s_floor;
+    // thread (q, rg): row q = tid mod 64 of the trailing matrix, columns r = rg + 16 m
+    const int qq = tid & 63, rg = tid >> 6;
     for (int p = 0; p < k; ++p) {
-        // every thread derives the pivot itself
-        double d = A[p + p * k];
-        const bool clamp = !(d > s_floor);
-        if (clamp) d = s_floor;
-        const double piv = sqrt(d);
-        __syncthreads();  // all have read A[p][p] before it is overwritten
-        if (tid == 0) {
-            A[p + p * k] = piv;
-            if (clamp && nclamp) atomicAdd(nclamp, 1);
+        double d = A[p + p * ld];
+        const bool clamp = !(d > fl);
+        if (clamp) d = fl;
+        const double inv = rsqrt(d);  // one reciprocal square root on the pivot chain
+        const double piv = d * inv;
+        // step p reads row p and writes rows > p of A and row p of R: one barrier per pivot
+        if (qq > p && qq < k) {
+            const double apq = A[p + qq * ld] * inv;
+            const int r0 = p + 1 + ((rg - (p + 1)) & 15);  // first r >= p + 1 with r = rg mod 16
+            for (int r = r0; r < k; r += 16)
+                if (r >= qq) A[qq + r * ld] -= apq * (A[p + r * ld] * inv);
         }
-        const double inv = 1.0 / piv;
-        // trailing update of the upper triangle with the scaled row p, then the row itself
-        const int w = k - p - 1;
-        for (int e = tid; e < w * w; e += blockDim.x) {
-            const int q = p + 1 + e / w, r = p + 1 + e % w;
-            if (q <= r) A[q + r * k] -= (A[p + q * k] * inv) * (A[p + r * k] * inv);
-        }
-        __syncthreads();  // the trailing update has read row p
-        for (int q = p + 1 + tid; q < k; q += blockDim.x) A[p + q * k] *= inv;
+        if (tid >= p && tid < k) R[p + tid * ld] = tid == p ? piv : A[p + tid * ld] * inv;
+        if (tid == 0 && clamp && nclamp) atomicAdd(nclamp, 1);
         __syncthreads();
     }
-    // inverse of the upper-triangular R, one column per thread (back substitution)
-    for (int jj = tid; jj < k; jj += blockDim.x) {
-        for (int i = k - 1; i >= 0; --i) {
-            double x = 0.0;
-            if (i <= jj) {
-                double acc = i == jj ? 1.0 : 0.0;
-                for (int l = i + 1; l <= jj; ++l) acc -= A[i + l * k] * B[l + jj * k];
-                x = acc / A[i + i * k];
-            }
-            B[i + jj * k] = x;
-        }
-    }
+    for (int i = tid; i < k; i += blockDim.x) s_rinv[i] = 1.0 / R[i + i * ld];
     __syncthreads();
+    // column jj of R^-1: x = e_jj; for l = jj .. 0: x_l /= R_ll, x_i -= R_il x_l (i < l);
+    // lane holds rows lane and lane + 32
+    for (int jj = warp; jj < k; jj += nwarp) {
+        double x0 = lane == jj ? 1.0 : 0.0, x1 = lane + 32 == jj ? 1.0 : 0.0;
+        for (int l = jj; l >= 0; --l) {
+            const double xl = __shfl_sync(0xFFFFFFFFu, l < 32 ? x0 : x1, l & 31) * s_rinv[l];
+            if (lane == (l & 31)) {
+                if (l < 32) x0 = xl;
+                else x1 = xl;
+            }
+            if (lane < l) x0 -= R[lane + l * ld] * xl;
+            if (lane + 32 < l) x1 -= R[lane + 32 + l * ld] * xl;
+        }
+        if (lane < k) Rinv[lane + jj * k] = lane <= jj ? x0 : 0.0;
+        if (lane + 32 < k) Rinv[lane + 32 + jj * k] = lane + 32 <= jj ? x1 : 0.0;
+    }
     for (int e = tid; e < k * k; e += blockDim.x) {
         const int i = e % k, jj = e / k;
-        Rout[i + (int64_t)jj * ldr] = A[e];
-        Rinv[e] = B[e];
+        Rout[i + (int64_t)jj * ldr] = R[i + jj * ld];
     }
 }
 
@@ -129,13 +145,26 @@ __global__ void k_trmm_upper(const double* __restrict__ A, int lda, const double
     }
 }
 
-// G = sum_b P[b] of nb partial matrices of kk entries each (a fixed summation order)
-__global__ void k_sum_partials(const double* __restrict__ P, int nb, int kk, double* __restrict__ G) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= kk) return;
+// G = sum_b P[b] of nb partial matrices of kk entries each, in a fixed order: CTAs of 256
+// threads take 32 consecutive entries, thread (e, sp) sums the partials b = sp mod 8 and the
+// eight split sums are added in order.
+__global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__ P, int nb, int kk,
+                                                      double* __restrict__ G) {
+    __shared__ double part[8][32];
+    const int c = threadIdx.x & 31, sp = threadIdx.x >> 5;
+    const int e = blockIdx.x * 32 + c;
     double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += P[(int64_t)b * kk + e];
-    G[e] = s;
+    if (e < kk) {
+#pragma unroll 4
+        for (int b = sp; b < nb; b += 8) s += P[(int64_t)b * kk + e];
+    }
+    part[sp][c] = s;
+    __syncthreads();
+    if (sp == 0 && e < kk) {
+        double t = part[0][c];
+        for (int q = 1; q < 8; ++q) t += part[q][c];
+        G[e] = t;
+    }
 }
 
 // Xa[i][a] = X[i][idx[a]] (node-major, X n x k, Xa n x ka)
@@ -279,68 +308,216 @@ __global__ void k_bhess_qr_step(double* __restrict__ H, int ldh, double* __restr
     }
 }
 
-// k_bhess_qr_step with its tiles in shared memory, for k <= 64 (dynamic shared memory
-// 4 k^2 + k doubles): the earlier reflectors are applied block by block to the 2k x k tile of
-// the new block column that each block touches, then the new block's reflectors are formed on
-// its own 2k x k tile together with the matching rows of the right-hand sides.
-__global__ void k_bhess_qr_step_smem(double* __restrict__ H, int ldh, double* __restrict__ tau,
-                                     double* __restrict__ Gv, int ldg, int k, int j, double* __restrict__ resid) {
+// The two kernels below split k_bhess_qr_step for k <= 64.
+//
+// k_bhess_apply_prev: the reflectors of block columns 0 .. j - 1 applied to block column j.
+// The new block's columns are independent: warp q of the grid owns column c0 + q and keeps a
+// 2k-row window of it in registers (local row lane + 32 s), the window of earlier block b
+// covering rows b k .. b k + 2k - 1. Block b's reflectors come through shared memory
+// (double-buffered by cp.async while the previous block is applied); v is read with the
+// unit diagonal and the zeros outside rows t .. t + k put in place. After block b the rows
+// b k .. b k + k - 1 are final and written back and the window moves down by k rows.
+// Dynamic shared memory: 2 (2k k + k) + (blockDim.x / 32) k doubles. Launched only for j > 0.
+__global__ void __launch_bounds__(256) k_bhess_apply_prev(double* __restrict__ H, int ldh,
+                                                          const double* __restrict__ tau, int k, int j) {
     extern __shared__ double sm[];
     const int k2 = 2 * k;
-    double* T = sm;           // 2k x k, ld 2k
-    double* V = T + k2 * k;   // 2k x k, ld 2k: reflectors of block b, then the right-hand-side rows
-    double* tb = V + k2 * k;  // k taus
-    __shared__ double red[256];
-    __shared__ double s_tau, s_scale;
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    double* stage = sm + 2 * k2 * k + 2 * k + warp * k;
+    const int q = blockIdx.x * nwarp + warp;
+    const bool own = q < k;
     const int c0 = j * k;
-    const int G = group_width(k), sub = tid % G, grp = tid / G, ngrp = blockDim.x / G;
-    for (int b = 0; b < j; ++b) {
+    double* col = H + (int64_t)(c0 + (own ? q : 0)) * ldh;
+    auto prefetch = [&](int b, int buf) {
         const int r0 = b * k;
-        for (int e = tid; e < k2 * k; e += blockDim.x) {
+        for (int e = threadIdx.x; e < k2 * k; e += blockDim.x) {
             const int i = e % k2, t = e / k2;
-            T[e] = H[(r0 + i) + (int64_t)(c0 + t) * ldh];
-            V[e] = H[(r0 + i) + (int64_t)(r0 + t) * ldh];
+            cp_async8(sm + buf * k2 * k + e, H + (r0 + i) + (int64_t)(r0 + t) * ldh);
         }
-        for (int t = tid; t < k; t += blockDim.x) tb[t] = tau[r0 + t];
+        for (int t = threadIdx.x; t < k; t += blockDim.x) cp_async8(sm + 2 * k2 * k + buf * k + t, tau + r0 + t);
+        cp_async_commit();
+    };
+    double x[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int i = lane + 32 * s;
+        x[s] = own && i < k2 ? col[i] : 0.0;
+    }
+    prefetch(0, 0);
+    for (int b = 0; b < j; ++b) {
+        const int r0 = b * k, buf = b & 1;
+        if (b + 1 < j) {
+            prefetch(b + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         __syncthreads();
-        // each group owns one column of T and applies the block's reflectors to it in order
-        for (int t = 0; t < k; ++t) {
-            const double tc = tb[t];
-            if (tc == 0.0) continue;
-            for (int q0 = 0; q0 < k; q0 += ngrp) {
-                const int q = q0 + grp;
-                apply_reflector(V + t * k2, tc, q < k ? T + q * k2 : nullptr, t, k, G, sub);
+        if (own) {
+            const double* V = sm + buf * k2 * k;
+            const double* tb = sm + 2 * k2 * k + buf * k;
+            for (int t = 0; t < k; ++t) {
+                const double tc = tb[t];
+                if (tc == 0.0) continue;
+                double v[4], part = 0.0;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int i = lane + 32 * s;
+                    const double raw = i < k2 ? V[t * k2 + i] : 0.0;
+                    v[s] = i < t || i > t + k ? 0.0 : (i == t ? 1.0 : raw);
+                    part += v[s] * x[s];
+                }
+                const double sc = warp_sum_d(part) * tc;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) x[s] -= sc * v[s];
+            }
+            if (b + 1 == j) {
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int i = lane + 32 * s;
+                    if (i < k2) col[r0 + i] = x[s];
+                }
+            } else {
+                // rows r0 .. r0 + k - 1 are final; the window moves down by k rows
+                double* st = stage;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int i = lane + 32 * s;
+                    if (i < k) col[r0 + i] = x[s];
+                    else if (i < k2) st[i - k] = x[s];
+                }
+                __syncwarp();
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int i = lane + 32 * s;
+                    x[s] = i < k ? st[i] : (i < k2 ? col[r0 + k + i] : 0.0);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();  // buffer buf is free for block b + 2
+    }
+}
+
+// Sum over the 8 lanes of a column group (lanes 8 c .. 8 c + 7 of a warp).
+__device__ __forceinline__ double group8_sum(double v) {
+    v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
+    v += __shfl_xor_sync(0xFFFFFFFFu, v, 2);
+    v += __shfl_xor_sync(0xFFFFFFFFu, v, 4);
+    return v;
+}
+
+// k_bhess_qr_tile: the new block's reflectors on its 2k x k tile (rows c0 .. c0 + 2k - 1 of
+// block column j, after k_bhess_apply_prev) together with the same rows of the k right-hand
+// sides Gv, and every right-hand side's residual. One CTA of 512 threads: column group
+// G = 4 warp + lane / 8 (8 lanes) holds tile column G and right-hand side G in registers,
+// lane g = lane mod 8 the local rows g + 8 r (r < 16). For reflector t the group of column t
+// forms it (LAPACK dlarfg convention, as reflect_column) and publishes v through shared
+// memory; after one barrier every group applies it to its columns right of t, touching only
+// the row slots that meet the reflector's rows t .. t + k.
+__global__ void __launch_bounds__(512) k_bhess_qr_tile(double* __restrict__ H, int ldh, double* __restrict__ tau,
+                                                       double* __restrict__ Gv, int ldg, int k, int j,
+                                                       double* __restrict__ resid) {
+    constexpr int NR = 16;
+    __shared__ double vbuf[2][128];
+    __shared__ double tbuf[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane & 7, cg = lane >> 3;
+    const int G = 4 * warp + cg;
+    const bool live = G < k;
+    const int c0 = j * k, k2 = 2 * k;
+    double x[2][NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int i = g + 8 * r;
+        const bool in = live && i < k2;
+        x[0][r] = in ? H[(c0 + i) + (int64_t)(c0 + G) * ldh] : 0.0;
+        x[1][r] = in ? Gv[(c0 + i) + (int64_t)G * ldg] : 0.0;
+    }
+    for (int t = 0; t < k; ++t) {
+        double* vb = vbuf[t & 1];
+        if (warp == (t >> 2)) {
+            // every group of the warp reduces its own column; only the group of column t keeps it.
+            // Rows below t + k of column t are zero (the lower block is triangular and the earlier
+            // reflectors end above row t + k), so the tail sum runs over all rows below t.
+            const bool og = cg == (t & 3);
+            double s0 = 0.0, s1 = 0.0, al = 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; r += 2) {
+                const int i0 = g + 8 * r, i1 = i0 + 8;
+                const double a0 = i0 > t ? x[0][r] : 0.0, a1 = i1 > t ? x[0][r + 1] : 0.0;
+                s0 += a0 * a0;
+                s1 += a1 * a1;
+                al = i0 == t ? x[0][r] : al;
+                al = i1 == t ? x[0][r + 1] : al;
+            }
+            const double sg = group8_sum(s0 + s1);
+            al = group8_sum(al);
+            double tc = 0.0, scale = 0.0, beta = al;
+            if (sg != 0.0) {
+                const double q = fma(al, al, sg);
+                const double rq = rsqrt(q);  // 1 / mu
+                const double mu = q * rq;
+                beta = al <= 0.0 ? mu : -mu;
+                const double d = al - beta;
+                tc = al <= 0.0 ? -d * rq : d * rq;  // (beta - al) / beta
+                scale = __drcp_rn(d);
+            }
+            if (og) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    const int i = g + 8 * r;  // all 128 rows: zeros below row 2k keep the padding inert
+                    const bool tail = i > t && i <= t + k && tc != 0.0;
+                    const double xs = tail ? x[0][r] * scale : x[0][r];
+                    x[0][r] = i == t ? beta : xs;
+                    vb[i] = i == t ? 1.0 : (tail ? xs : 0.0);
+                }
+                if (g == 0) {
+                    tbuf[t & 1] = tc;
+                    tau[c0 + t] = tc;
+                }
             }
         }
         __syncthreads();
-        for (int e = tid; e < k2 * k; e += blockDim.x) {
-            const int i = e % k2, t = e / k2;
-            H[(r0 + i) + (int64_t)(c0 + t) * ldh] = T[e];
+        const double tc = tbuf[t & 1];
+        if (tc != 0.0) {  // uniform: every lane takes part in the shuffles (idle groups hold zeros)
+            // v is zero outside rows t .. t + k, so all row slots are summed without tests
+            double v[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) v[r] = vb[g + 8 * r];
+            double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; r += 2) {
+                a0 = fma(v[r], x[0][r], a0);
+                a1 = fma(v[r + 1], x[0][r + 1], a1);
+                b0 = fma(v[r], x[1][r], b0);
+                b1 = fma(v[r + 1], x[1][r + 1], b1);
+            }
+            const double p0 = group8_sum(a0 + a1), p1 = group8_sum(b0 + b1);
+            const double f0 = live && G > t ? p0 * tc : 0.0, f1 = live ? p1 * tc : 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                x[0][r] = fma(-f0, v[r], x[0][r]);
+                x[1][r] = fma(-f1, v[r], x[1][r]);
+            }
         }
-        __syncthreads();
     }
-    for (int e = tid; e < k2 * k; e += blockDim.x) {
-        const int i = e % k2, t = e / k2;
-        T[e] = H[(c0 + i) + (int64_t)(c0 + t) * ldh];
-        V[e] = Gv[(c0 + i) + (int64_t)t * ldg];
+    // the store addresses are formed afresh (opaque copies of the bases and strides), so the
+    // load addresses are not kept live through the reflector loop
+    double* Hs = H;
+    double* Gs = Gv;
+    int ldhs = ldh, ldgs = ldg;
+    asm volatile("" : "+l"(Hs), "+l"(Gs), "+r"(ldhs), "+r"(ldgs));
+    double rs = 0.0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int i = g + 8 * r;
+        if (!live || i >= k2) continue;
+        Hs[(c0 + i) + (int64_t)(c0 + G) * ldhs] = x[0][r];
+        Gs[(c0 + i) + (int64_t)G * ldgs] = x[1][r];
+        if (i >= k) rs += x[1][r] * x[1][r];
     }
-    __syncthreads();
-    for (int t0 = 0; t0 < k; ++t0) {
-        const double tc = reflect_column(T, k2, V, k2, t0, k, red, &s_tau, &s_scale, G, sub, grp, ngrp);
-        if (tid == 0) tau[c0 + t0] = tc;
-    }
-    for (int e = tid; e < k2 * k; e += blockDim.x) {
-        const int i = e % k2, t = e / k2;
-        H[(c0 + i) + (int64_t)(c0 + t) * ldh] = T[e];
-        Gv[(c0 + i) + (int64_t)t * ldg] = V[e];
-    }
-    for (int a = tid; a < k; a += blockDim.x) {
-        const double* g = V + a * k2;
-        double s = 0.0;
-        for (int i = k; i < k2; ++i) s += g[i] * g[i];
-        resid[a] = sqrt(s);
-    }
+    rs = group8_sum(rs);
+    if (live && g == 0) resid[G] = sqrt(rs);
 }
 
 }  // namespace bie

@@ -864,15 +864,19 @@ void gram(bie_geom* g, cublasHandle_t h, const double* Q, int ka, int64_t n, dou
         blas_ck(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, ka, ka, (int)rem, &one, Q + nfull * c * ka, ka,
                             Q + nfull * c * ka, ka, &zero, P + nfull * kk, ka),
                 "gemm");
-    k_sum_partials<<<grid1(kk), 256, 0, s>>>(P, nb, (int)kk, G);
+    k_sum_partials<<<(unsigned)((kk + 31) / 32), 256, 0, s>>>(P, nb, (int)kk, G);
     BIE_CK(cudaGetLastError());
 }
 
 // Orthonormalises the rows of Q (ka x n, column-major, ld ka: the transposed block of ka
-// vectors) by Cholesky QR applied twice: Q_old = R^T Q_new, R = R2 R1 (ka x ka upper) into
-// Rout (ld ldr). Up to 64 columns the Gram matrix comes from chunked DGEMMs, is factored and
-// inverted in shared memory and applied as a DGEMM with R^-T; wider blocks use SYRK and TRSM.
-void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double* Rout, int ldr, cudaStream_t s) {
+// vectors) by Cholesky QR applied `passes` times (2: CholQR2, orthogonal to working precision
+// for condition numbers up to about 1e8; 1: orthogonality error about cond^2 1e-16, enough
+// for the reduced-precision inner solves that stop near 1e-6): Q_old = R^T Q_new, R = R2 R1
+// (ka x ka upper) into Rout (ld ldr). Up to 64 columns the Gram matrix comes from chunked
+// DGEMMs, is factored and inverted in shared memory and applied as a DGEMM with R^-T; wider
+// blocks use SYRK and TRSM.
+void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double* Rout, int ldr, cudaStream_t s,
+             int passes = 2) {
     const double one = 1.0, zero = 0.0;
     double* R1 = g->br1.as<double>();
     double* R2 = g->br2.as<double>();
@@ -882,19 +886,19 @@ void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double
         double* Gm = g->br.as<double>();
         double* Ri = g->binv.as<double>();
         double* tmp = g->btmp.as<double>();
-        const size_t sm = 2 * sizeof(double) * (size_t)ka * ka;
+        const size_t sm = 2 * sizeof(double) * (size_t)ka * (ka + 1);
         ensure_smem_limit((const void*)k_chol_inv_smem, sm);
-        for (int pass = 0; pass < 2; ++pass) {
+        for (int pass = 0; pass < passes; ++pass) {
             double* Rp = pass == 0 ? R1 : R2;
             gram(g, h, Q, ka, n, Gm, s);
-            k_chol_inv_smem<<<1, 256, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
+            k_chol_inv_smem<<<1, 1024, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
             BIE_CK(cudaGetLastError());
             blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, ka, &one, Ri, ka, Q, ka, &zero, tmp, ka),
                     "gemm");
             BIE_CK(cudaMemcpyAsync(Q, tmp, sizeof(double) * (size_t)n * ka, cudaMemcpyDeviceToDevice, s));
         }
     } else {
-        for (int pass = 0; pass < 2; ++pass) {
+        for (int pass = 0; pass < passes; ++pass) {
             double* Rp = pass == 0 ? R1 : R2;
             blas_ck(cublasDsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, ka, (int)n, &one, Q, ka, &zero, Rp, ka),
                     "syrk");
@@ -905,6 +909,11 @@ void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double
                     "trsm");
         }
     }
+    if (passes == 1) {
+        BIE_CK(cudaMemcpy2DAsync(Rout, sizeof(double) * (size_t)ldr, R1, sizeof(double) * (size_t)ka,
+                                 sizeof(double) * (size_t)ka, (size_t)ka, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
     k_trmm_upper<<<grid1((int64_t)ka * ka), 256, 0, s>>>(R2, ka, R1, ka, Rout, ldr, ka);
     BIE_CK(cudaGetLastError());
 }
@@ -912,7 +921,8 @@ void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double
 // Block GMRES (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285): the active
 // columns of dr share one block Krylov space. Block Arnoldi with classical Gram-Schmidt
 // against the whole basis (two passes for FP64 solves, one for the reduced-precision inner
-// solves), each new block orthonormalised by Cholesky QR applied twice; the block
+// solves), each new block orthonormalised by Cholesky QR (twice for FP64 solves, once for
+// the inner solves); the block
 // upper-Hessenberg least-squares problem is updated by Householder reflections one block
 // column per iteration, which gives every column's residual norm. The tall-skinny products
 // with the basis are cuBLAS DGEMMs. The basis is kept as the rows of M ((m + 1) ka x n,
@@ -989,7 +999,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         // V_0 S_0 = R (Cholesky QR); Gv = [S_0; 0]
         {
             Prof pf(g, BIE_KERNEL_KRYLOV, s);
-            cholqr2(g, h, Ra, ka, n, Gv, (int)L, s);
+            cholqr2(g, h, Ra, ka, n, Gv, (int)L, s, one_pass ? 1 : 2);
             BIE_CK(cudaMemcpy2DAsync(M, pitchL, Ra, pitchK, pitchK, (size_t)n, cudaMemcpyDeviceToDevice, s));
         }
         int jend = 0;
@@ -1022,15 +1032,21 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                             "geam");
                 }
                 // the new block: W = V_{j+1} R, R into H's block (j + 1, j)
-                cholqr2(g, h, Q, ka, n, Hc + rows, (int)L, s);
+                cholqr2(g, h, Q, ka, n, Hc + rows, (int)L, s, one_pass ? 1 : 2);
                 BIE_CK(cudaMemcpy2DAsync(M + (size_t)(j + 1) * ka, pitchL, Q, pitchK, pitchK, (size_t)n,
                                          cudaMemcpyDeviceToDevice, s));
                 // least squares: the Householder QR of block column j and every column's residual
                 if (ka <= 64) {
-                    const size_t sm = sizeof(double) * (4 * (size_t)ka * ka + ka);
-                    ensure_smem_limit((const void*)k_bhess_qr_step_smem, sm);
-                    k_bhess_qr_step_smem<<<1, 256, sm, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
-                                                            g->bres.as<double>());
+                    if (j > 0) {
+                        const int nw = 8;
+                        const size_t sm = sizeof(double) * (2 * (2 * (size_t)ka * ka + ka) + (size_t)nw * ka);
+                        ensure_smem_limit((const void*)k_bhess_apply_prev, sm);
+                        k_bhess_apply_prev<<<(ka + nw - 1) / nw, 32 * nw, sm, s>>>(H, (int)L, g->btau.as<double>(),
+                                                                                   ka, j);
+                        BIE_CK(cudaGetLastError());
+                    }
+                    k_bhess_qr_tile<<<1, 512, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
+                                                      g->bres.as<double>());
                 } else {
                     k_bhess_qr_step<<<1, 256, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
                                                       g->bres.as<double>());
