@@ -772,8 +772,9 @@ def main():
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--block", type=int, default=0, choices=[0, 1],
-                    help="1: block GMRES (one Krylov space shared by the block's columns)")
+    ap.add_argument("--block", type=int, default=1, choices=[0, 1],
+                    help="1 (default): block GMRES, one Krylov space shared by the block's columns, the "
+                         "method of solve_dielectric_box3d_block; 0: one Arnoldi process per column")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-stream measurement")
     ap.add_argument("--profile-matvec", action="store_true",
                     help="apply the refined and the FP64 operator once each to k columns and exit "

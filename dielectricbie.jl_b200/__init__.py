@@ -861,14 +861,16 @@ def solve_gmres(A: GPUDielectricOperator, b, atol: float = 1e-6, rtol: float = 1
 def solve_dielectric_box3d_block(interface: DielectricInterface, sources, eps_src=None, *, fmm_tol: float = 1e-9,
                                  up_tol: float = 1e-9, max_order: int = 8, rtol: float = 1e-10, atol: float = 0.0,
                                  itmax: int = 500, precondition: bool = True, correct_edges: bool = True,
-                                 precision: str = "fp64", device: int = 0, **kw):
+                                 precision: str = "fp64", device: int = 0, block: bool = True, **kw):
     """``solve_dielectric_box3d_block`` (src/solver/multi_rhs.jl:270-286) for PointSource right-hand
     sides (the reference takes VolumeSources; the operator is the same). eps_src defaults to each
-    panel's eps_in of the first panel (source inside a single box). Returns (Sigma, stats)."""
+    panel's eps_in of the first panel (source inside a single box). block=True (the default) solves
+    the columns in one block Krylov space, as the reference's Krylov.block_gmres; block=False runs
+    one Arnoldi process per column. Returns (Sigma, stats)."""
     op = batched_lhs_dielectric_box3d_fmm3d_corrected(interface, fmm_tol, up_tol, max_order,
                                                       correct_edges=correct_edges, precision=precision,
                                                       device=device)
     if eps_src is None:
         eps_src = float(interface.eps_in[0])
     return gpu_solve_sources(op, list(sources), eps_src, rtol=rtol, atol=atol, itmax=itmax,
-                             precondition=precondition, **kw)
+                             precondition=precondition, block=block, **kw)

@@ -310,95 +310,6 @@ __global__ void k_bhess_qr_step(double* __restrict__ H, int ldh, double* __restr
 
 // The two kernels below split k_bhess_qr_step for k <= 64.
 //
-// k_bhess_apply_prev: the reflectors of block columns 0 .. j - 1 applied to block column j.
-// The new block's columns are independent: warp q of the grid owns column c0 + q and keeps a
-// 2k-row window of it in registers (local row lane + 32 s), the window of earlier block b
-// covering rows b k .. b k + 2k - 1. Block b's reflectors come through shared memory
-// (double-buffered by cp.async while the previous block is applied); v is read with the
-// unit diagonal and the zeros outside rows t .. t + k put in place. After block b the rows
-// b k .. b k + k - 1 are final and written back and the window moves down by k rows.
-// Dynamic shared memory: 2 (2k k + k) + (blockDim.x / 32) k doubles. Launched only for j > 0.
-__global__ void __launch_bounds__(256) k_bhess_apply_prev(double* __restrict__ H, int ldh,
-                                                          const double* __restrict__ tau, int k, int j) {
-    extern __shared__ double sm[];
-    const int k2 = 2 * k;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    double* stage = sm + 2 * k2 * k + 2 * k + warp * k;
-    const int q = blockIdx.x * nwarp + warp;
-    const bool own = q < k;
-    const int c0 = j * k;
-    double* col = H + (int64_t)(c0 + (own ? q : 0)) * ldh;
-    auto prefetch = [&](int b, int buf) {
-        const int r0 = b * k;
-        for (int e = threadIdx.x; e < k2 * k; e += blockDim.x) {
-            const int i = e % k2, t = e / k2;
-            cp_async8(sm + buf * k2 * k + e, H + (r0 + i) + (int64_t)(r0 + t) * ldh);
-        }
-        for (int t = threadIdx.x; t < k; t += blockDim.x) cp_async8(sm + 2 * k2 * k + buf * k + t, tau + r0 + t);
-        cp_async_commit();
-    };
-    double x[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const int i = lane + 32 * s;
-        x[s] = own && i < k2 ? col[i] : 0.0;
-    }
-    prefetch(0, 0);
-    for (int b = 0; b < j; ++b) {
-        const int r0 = b * k, buf = b & 1;
-        if (b + 1 < j) {
-            prefetch(b + 1, buf ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        if (own) {
-            const double* V = sm + buf * k2 * k;
-            const double* tb = sm + 2 * k2 * k + buf * k;
-            for (int t = 0; t < k; ++t) {
-                const double tc = tb[t];
-                if (tc == 0.0) continue;
-                double v[4], part = 0.0;
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int i = lane + 32 * s;
-                    const double raw = i < k2 ? V[t * k2 + i] : 0.0;
-                    v[s] = i < t || i > t + k ? 0.0 : (i == t ? 1.0 : raw);
-                    part += v[s] * x[s];
-                }
-                const double sc = warp_sum_d(part) * tc;
-#pragma unroll
-                for (int s = 0; s < 4; ++s) x[s] -= sc * v[s];
-            }
-            if (b + 1 == j) {
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int i = lane + 32 * s;
-                    if (i < k2) col[r0 + i] = x[s];
-                }
-            } else {
-                // rows r0 .. r0 + k - 1 are final; the window moves down by k rows
-                double* st = stage;
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int i = lane + 32 * s;
-                    if (i < k) col[r0 + i] = x[s];
-                    else if (i < k2) st[i - k] = x[s];
-                }
-                __syncwarp();
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int i = lane + 32 * s;
-                    x[s] = i < k ? st[i] : (i < k2 ? col[r0 + k + i] : 0.0);
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();  // buffer buf is free for block b + 2
-    }
-}
-
 // Sum over the 8 lanes of a column group (lanes 8 c .. 8 c + 7 of a warp).
 __device__ __forceinline__ double group8_sum(double v) {
     v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
@@ -407,20 +318,112 @@ __device__ __forceinline__ double group8_sum(double v) {
     return v;
 }
 
+// Doubles per block column in the compact-WY buffer: V (2k x k, ld 2k; unit diagonal and zeros
+// in place) followed by T^T (k x k, ld k), the total rounded up to an even count so that every
+// block starts on a 16-byte boundary.
+__host__ __device__ inline int wy_stride(int k) { return (2 * k * k + k * k + 1) & ~1; }
+
+// One reflector t of k_bhess_qr_tile, for t in 8 P .. 8 P + 7: reflector t spans rows
+// t .. t + k <= 8 P + 7 + 64, so only the row slots P .. P + 8 take part (compile-time range).
+template <int P>
+__device__ __forceinline__ void tile_reflector(double (&x)[2][16], int t, int k, int g, int cg, int warp, int G,
+                                               bool live, double* vbuf, double* tbuf, double* stau, double* U,
+                                               double* tau_out) {
+    constexpr int R0 = P, R1 = P + 8 < 15 ? P + 8 : 15;
+    double* vb = vbuf + (t & 1) * 128;
+    if (warp == (t >> 2)) {
+        // every group of the warp reduces its own column; only the group of column t keeps it.
+        // Rows below t + k of column t are zero (the lower block is triangular and the earlier
+        // reflectors end above row t + k), so the tail sum runs over all rows below t.
+        const bool og = cg == (t & 3);
+        double s0 = 0.0, s1 = 0.0, al = 0.0;
+#pragma unroll
+        for (int r = R0; r <= R1; ++r) {
+            const int i = g + 8 * r;
+            const double a = i > t ? x[0][r] : 0.0;
+            if (r & 1) s1 = fma(a, a, s1);
+            else s0 = fma(a, a, s0);
+            al = i == t ? x[0][r] : al;
+        }
+        const double sg = group8_sum(s0 + s1);
+        al = group8_sum(al);
+        double tc = 0.0, scale = 0.0, beta = al;
+        if (sg != 0.0) {
+            const double q = fma(al, al, sg);
+            const double rq = rsqrt(q);  // 1 / mu
+            const double mu = q * rq;
+            beta = al <= 0.0 ? mu : -mu;
+            const double d = al - beta;
+            tc = al <= 0.0 ? -d * rq : d * rq;  // (beta - al) / beta
+            scale = __drcp_rn(d);
+        }
+        if (og) {
+#pragma unroll
+            for (int r = R0; r <= R1; ++r) {
+                const int i = g + 8 * r;
+                const bool tail = i > t && i <= t + k && tc != 0.0;
+                const double xs = tail ? x[0][r] * scale : x[0][r];
+                x[0][r] = i == t ? beta : xs;
+                vb[i] = i == t ? 1.0 : (tail ? xs : 0.0);
+            }
+            if (g == 0) {
+                tbuf[t & 1] = tc;
+                stau[t] = tc;
+                tau_out[t] = tc;
+            }
+        }
+    }
+    __syncthreads();
+    const double tc = tbuf[t & 1];
+    if (tc != 0.0) {  // uniform: every lane takes part in the shuffles (idle groups hold zeros)
+        double v[R1 - R0 + 1];
+#pragma unroll
+        for (int r = R0; r <= R1; ++r) v[r - R0] = vb[g + 8 * r];
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+        for (int r = R0; r <= R1; ++r) {
+            if (r & 1) {
+                a1 = fma(v[r - R0], x[0][r], a1);
+                b1 = fma(v[r - R0], x[1][r], b1);
+            } else {
+                a0 = fma(v[r - R0], x[0][r], a0);
+                b0 = fma(v[r - R0], x[1][r], b0);
+            }
+        }
+        const double p0 = group8_sum(a0 + a1), p1 = group8_sum(b0 + b1);
+        if (live && G < t && g == 0) U[G + t * 65] = p0;
+        const double f0 = live && G > t ? p0 * tc : 0.0, f1 = live ? p1 * tc : 0.0;
+#pragma unroll
+        for (int r = R0; r <= R1; ++r) {
+            x[0][r] = fma(-f0, v[r - R0], x[0][r]);
+            x[1][r] = fma(-f1, v[r - R0], x[1][r]);
+        }
+    }
+}
+
 // k_bhess_qr_tile: the new block's reflectors on its 2k x k tile (rows c0 .. c0 + 2k - 1 of
 // block column j, after k_bhess_apply_prev) together with the same rows of the k right-hand
 // sides Gv, and every right-hand side's residual. One CTA of 512 threads: column group
 // G = 4 warp + lane / 8 (8 lanes) holds tile column G and right-hand side G in registers,
 // lane g = lane mod 8 the local rows g + 8 r (r < 16). For reflector t the group of column t
 // forms it (LAPACK dlarfg convention, as reflect_column) and publishes v through shared
-// memory; after one barrier every group applies it to its columns right of t, touching only
-// the row slots that meet the reflector's rows t .. t + k.
+// memory; after one barrier every group applies it to its columns right of t, over the row
+// slots the reflector meets (tile_reflector; no data-dependent branches).
+//
+// The block's compact-WY form comes out as well: Q_j = H_0 .. H_{k-1} = I - V T V^T with
+// T = (strictly-upper(V^T V) + diag(1 / tau))^-1 (a zero tau gives a zero row and column of
+// T). The dot product group G < t forms for reflector t is (V^T V)[G][t], since its column
+// is final (v_G, with beta at row G where v_t is zero). V (unit diagonal and zeros in place)
+// and T^T (Tt[a + l k] = T[l][a]) are written to wy (wy_stride(k) doubles).
 __global__ void __launch_bounds__(512) k_bhess_qr_tile(double* __restrict__ H, int ldh, double* __restrict__ tau,
                                                        double* __restrict__ Gv, int ldg, int k, int j,
-                                                       double* __restrict__ resid) {
-    constexpr int NR = 16;
-    __shared__ double vbuf[2][128];
+                                                       double* __restrict__ resid, double* __restrict__ wy) {
+    constexpr int NR = 16, LDU = 65;
+    __shared__ double vbuf[2 * 128];
     __shared__ double tbuf[2];
+    __shared__ double stau[64];
+    __shared__ double U[64 * LDU];  // strictly upper part of V^T V, column-major
+    for (int e = threadIdx.x; e < 64 * LDU; e += blockDim.x) U[e] = 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane & 7, cg = lane >> 3;
     const int G = 4 * warp + cg;
     const bool live = G < k;
@@ -433,80 +436,31 @@ __global__ void __launch_bounds__(512) k_bhess_qr_tile(double* __restrict__ H, i
         x[0][r] = in ? H[(c0 + i) + (int64_t)(c0 + G) * ldh] : 0.0;
         x[1][r] = in ? Gv[(c0 + i) + (int64_t)G * ldg] : 0.0;
     }
+    __syncthreads();  // U cleared
     for (int t = 0; t < k; ++t) {
-        double* vb = vbuf[t & 1];
-        if (warp == (t >> 2)) {
-            // every group of the warp reduces its own column; only the group of column t keeps it.
-            // Rows below t + k of column t are zero (the lower block is triangular and the earlier
-            // reflectors end above row t + k), so the tail sum runs over all rows below t.
-            const bool og = cg == (t & 3);
-            double s0 = 0.0, s1 = 0.0, al = 0.0;
-#pragma unroll
-            for (int r = 0; r < NR; r += 2) {
-                const int i0 = g + 8 * r, i1 = i0 + 8;
-                const double a0 = i0 > t ? x[0][r] : 0.0, a1 = i1 > t ? x[0][r + 1] : 0.0;
-                s0 += a0 * a0;
-                s1 += a1 * a1;
-                al = i0 == t ? x[0][r] : al;
-                al = i1 == t ? x[0][r + 1] : al;
-            }
-            const double sg = group8_sum(s0 + s1);
-            al = group8_sum(al);
-            double tc = 0.0, scale = 0.0, beta = al;
-            if (sg != 0.0) {
-                const double q = fma(al, al, sg);
-                const double rq = rsqrt(q);  // 1 / mu
-                const double mu = q * rq;
-                beta = al <= 0.0 ? mu : -mu;
-                const double d = al - beta;
-                tc = al <= 0.0 ? -d * rq : d * rq;  // (beta - al) / beta
-                scale = __drcp_rn(d);
-            }
-            if (og) {
-#pragma unroll
-                for (int r = 0; r < NR; ++r) {
-                    const int i = g + 8 * r;  // all 128 rows: zeros below row 2k keep the padding inert
-                    const bool tail = i > t && i <= t + k && tc != 0.0;
-                    const double xs = tail ? x[0][r] * scale : x[0][r];
-                    x[0][r] = i == t ? beta : xs;
-                    vb[i] = i == t ? 1.0 : (tail ? xs : 0.0);
-                }
-                if (g == 0) {
-                    tbuf[t & 1] = tc;
-                    tau[c0 + t] = tc;
-                }
-            }
+#define BIE_TILE_PHASE(P)                                                                                  \
+    case P:                                                                                                \
+        tile_reflector<P>(x, t, k, g, cg, warp, G, live, vbuf, tbuf, stau, U, tau + c0);                  \
+        break;
+        switch (t >> 3) {
+            BIE_TILE_PHASE(0)
+            BIE_TILE_PHASE(1)
+            BIE_TILE_PHASE(2)
+            BIE_TILE_PHASE(3)
+            BIE_TILE_PHASE(4)
+            BIE_TILE_PHASE(5)
+            BIE_TILE_PHASE(6)
+            BIE_TILE_PHASE(7)
         }
-        __syncthreads();
-        const double tc = tbuf[t & 1];
-        if (tc != 0.0) {  // uniform: every lane takes part in the shuffles (idle groups hold zeros)
-            // v is zero outside rows t .. t + k, so all row slots are summed without tests
-            double v[NR];
-#pragma unroll
-            for (int r = 0; r < NR; ++r) v[r] = vb[g + 8 * r];
-            double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-#pragma unroll
-            for (int r = 0; r < NR; r += 2) {
-                a0 = fma(v[r], x[0][r], a0);
-                a1 = fma(v[r + 1], x[0][r + 1], a1);
-                b0 = fma(v[r], x[1][r], b0);
-                b1 = fma(v[r + 1], x[1][r + 1], b1);
-            }
-            const double p0 = group8_sum(a0 + a1), p1 = group8_sum(b0 + b1);
-            const double f0 = live && G > t ? p0 * tc : 0.0, f1 = live ? p1 * tc : 0.0;
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                x[0][r] = fma(-f0, v[r], x[0][r]);
-                x[1][r] = fma(-f1, v[r], x[1][r]);
-            }
-        }
+#undef BIE_TILE_PHASE
     }
     // the store addresses are formed afresh (opaque copies of the bases and strides), so the
     // load addresses are not kept live through the reflector loop
     double* Hs = H;
     double* Gs = Gv;
+    double* Ws = wy;
     int ldhs = ldh, ldgs = ldg;
-    asm volatile("" : "+l"(Hs), "+l"(Gs), "+r"(ldhs), "+r"(ldgs));
+    asm volatile("" : "+l"(Hs), "+l"(Gs), "+l"(Ws), "+r"(ldhs), "+r"(ldgs));
     double rs = 0.0;
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
@@ -514,10 +468,154 @@ __global__ void __launch_bounds__(512) k_bhess_qr_tile(double* __restrict__ H, i
         if (!live || i >= k2) continue;
         Hs[(c0 + i) + (int64_t)(c0 + G) * ldhs] = x[0][r];
         Gs[(c0 + i) + (int64_t)G * ldgs] = x[1][r];
+        Ws[i + G * k2] = i < G || i > G + k ? 0.0 : (i == G ? 1.0 : x[0][r]);
         if (i >= k) rs += x[1][r] * x[1][r];
     }
     rs = group8_sum(rs);
     if (live && g == 0) resid[G] = sqrt(rs);
+    __syncthreads();
+    // T = U^-1 (U with diagonal 1 / tau): column a by back substitution, x = e_a, for
+    // l = a .. 0: x_l *= tau_l, x_i -= U[i][l] x_l (i < l); warp w takes columns w + 16 m,
+    // interleaved; lane holds rows lane and lane + 32
+    double y0[4], y1[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int a = warp + 16 * m;
+        y0[m] = lane == a ? 1.0 : 0.0;
+        y1[m] = lane + 32 == a ? 1.0 : 0.0;
+    }
+    for (int l = k - 1; l >= 0; --l) {
+        const double tl = stau[l];
+        const double u0 = lane < l ? U[lane + l * LDU] : 0.0;
+        const double u1 = lane + 32 < l ? U[lane + 32 + l * LDU] : 0.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const double xl = __shfl_sync(0xFFFFFFFFu, l < 32 ? y0[m] : y1[m], l & 31) * tl;
+            if (lane == (l & 31)) {
+                if (l < 32) y0[m] = xl;
+                else y1[m] = xl;
+            }
+            y0[m] = fma(-u0, xl, y0[m]);
+            y1[m] = fma(-u1, xl, y1[m]);
+        }
+    }
+    double* Tt = Ws + k2 * k;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int a = warp + 16 * m;
+        if (a >= k) continue;
+        if (lane < k) Tt[a + lane * k] = lane <= a ? y0[m] : 0.0;
+        if (lane + 32 < k) Tt[a + (lane + 32) * k] = lane + 32 <= a ? y1[m] : 0.0;
+    }
+}
+
+// k_bhess_apply_prev: the reflectors of block columns 0 .. j - 1 applied to block column j as
+// compact-WY block reflectors, in order: on rows b k .. b k + 2k - 1,
+//   C <- Q_b^T C = C - V_b T_b^T (V_b^T C)
+// with V_b the block's unit lower-trapezoidal reflectors (column t nonzero on rows t .. t + k)
+// and T_b^T, both from k_bhess_qr_tile (wy + b wy_stride(k)). Each CTA (256 threads) takes
+// kApplyCols columns of the block column and keeps their 2k-row window in shared memory; the
+// next block's V and T^T are copied by cp.async (16-byte pieces) while the current one is
+// applied. Three barrier-separated products per block: W = V^T C (k x NC), W2 = T^T W,
+// C -= V W2, each sum over the rows where V is nonzero. After block b the window's top k rows
+// are final and written back and the window moves down by k rows. Launched only for j > 0;
+// k <= 64.
+constexpr int kApplyCols = 4;
+inline size_t apply_prev_smem(int k) {
+    return sizeof(double) * (2 * (size_t)wy_stride(k) + 4 * (size_t)k * kApplyCols);
+}
+__global__ void __launch_bounds__(256) k_bhess_apply_prev(double* __restrict__ H, int ldh,
+                                                          const double* __restrict__ wy, int k, int j) {
+    constexpr int NC = kApplyCols;
+    extern __shared__ double sm[];
+    const int k2 = 2 * k, bs = wy_stride(k), tid = threadIdx.x;
+    double* C = sm + 2 * bs;  // 2k x NC (ld 2k)
+    double* W = C + k2 * NC;  // k x NC (ld k)
+    double* W2 = W + k * NC;  // k x NC (ld k)
+    const int q0 = blockIdx.x * NC, nc = min(NC, k - q0);
+    const int c0 = j * k;
+    auto colp = [&](int c) { return H + (int64_t)(c0 + q0 + c) * ldh; };
+    auto prefetch = [&](int b, int buf) {
+        const double* src = wy + (int64_t)b * bs;
+        double* dst = sm + buf * bs;
+        for (int e = 2 * tid; e < bs; e += 2 * blockDim.x) cp_async16(dst + e, src + e);
+        cp_async_commit();
+    };
+    for (int c = 0; c < NC; ++c)
+        for (int i = tid; i < k2; i += blockDim.x) C[i + c * k2] = c < nc ? colp(c)[i] : 0.0;
+    prefetch(0, 0);
+    for (int b = 0; b < j; ++b) {
+        const int r0 = b * k, buf = b & 1;
+        if (b + 1 < j) {
+            prefetch(b + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double* V = sm + buf * bs;
+        const double* T = V + k2 * k;
+        // W = V^T C: W[t][c] = sum over i = t .. t + k of V[i][t] C[i][c]
+        for (int o = tid; o < k * NC; o += blockDim.x) {
+            const int c = o / k, t = o - c * k;
+            const double* v = V + t * k2 + t;
+            const double* x = C + c * k2 + t;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int i = 0;
+            for (; i + 3 <= k; i += 4) {
+                a0 = fma(v[i], x[i], a0);
+                a1 = fma(v[i + 1], x[i + 1], a1);
+                a2 = fma(v[i + 2], x[i + 2], a2);
+                a3 = fma(v[i + 3], x[i + 3], a3);
+            }
+            for (; i <= k; ++i) a0 = fma(v[i], x[i], a0);
+            W[t + c * k] = (a0 + a1) + (a2 + a3);
+        }
+        __syncthreads();
+        // W2 = T^T W: W2[a][c] = sum over l <= a of T[l][a] W[l][c]  (T^T stored: T[a + l k] = T[l][a])
+        for (int o = tid; o < k * NC; o += blockDim.x) {
+            const int c = o / k, a = o - c * k;
+            const double* w = W + c * k;
+            double a0 = 0.0, a1 = 0.0;
+            int l = 0;
+            for (; l + 1 <= a; l += 2) {
+                a0 = fma(T[a + l * k], w[l], a0);
+                a1 = fma(T[a + (l + 1) * k], w[l + 1], a1);
+            }
+            if (l == a) a0 = fma(T[a + l * k], w[l], a0);
+            W2[a + c * k] = a0 + a1;
+        }
+        __syncthreads();
+        // C -= V W2: C[i][c] -= sum over t = max(0, i - k) .. min(i, k - 1) of V[i][t] W2[t][c]
+        for (int o = tid; o < k2 * NC; o += blockDim.x) {
+            const int c = o / k2, i = o - c * k2;
+            const int t0 = max(0, i - k), t1 = min(i, k - 1);
+            const double* w = W2 + c * k;
+            double a0 = 0.0, a1 = 0.0;
+            int t = t0;
+            for (; t + 1 <= t1; t += 2) {
+                a0 = fma(V[i + t * k2], w[t], a0);
+                a1 = fma(V[i + (t + 1) * k2], w[t + 1], a1);
+            }
+            if (t == t1) a0 = fma(V[i + t * k2], w[t], a0);
+            C[o] -= a0 + a1;
+        }
+        __syncthreads();
+        if (b + 1 == j) {
+            for (int c = 0; c < nc; ++c)
+                for (int i = tid; i < k2; i += blockDim.x) colp(c)[r0 + i] = C[i + c * k2];
+        } else {
+            // rows r0 .. r0 + k - 1 are final; the window moves down by k rows
+            for (int c = 0; c < nc; ++c)
+                for (int i = tid; i < k; i += blockDim.x) {
+                    double* x = C + c * k2;
+                    colp(c)[r0 + i] = x[i];
+                    x[i] = x[i + k];
+                    x[i + k] = colp(c)[r0 + 2 * k + i];
+                }
+        }
+        __syncthreads();  // the window is complete and buffer buf is free for block b + 2
+    }
 }
 
 }  // namespace bie

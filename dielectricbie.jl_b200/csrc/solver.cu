@@ -37,7 +37,7 @@ struct bie_geom {
     // solver workspace
     bie::Buf V, W, R, gv, cs, sn, h, h2, hn, beta, eps, active, jlast, yv, resid, dpart, rr, xo, dd, io_a, io_b, sol;
     // block GMRES workspace: basis, Hessenberg matrix, right-hand sides, small factors
-    bie::Buf bv, bq, bvj, bh, bgv, btau, br1, br2, br, bh2, bres, bidx, bflag, xa, ra, binv, bpart, btmp;
+    bie::Buf bv, bq, bvj, bh, bgv, btau, br1, br2, br, bh2, bres, bidx, bflag, xa, ra, binv, bpart, btmp, bwy;
     cublasHandle_t blas = nullptr;  // created on the first block solve
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // kernel timing
@@ -958,6 +958,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
     g->bh.ensure(sizeof(double) * (size_t)L * m * ka);
     g->bgv.ensure(sizeof(double) * (size_t)L * ka);
     g->btau.ensure(sizeof(double) * (size_t)m * ka);
+    if (ka <= 64) g->bwy.ensure(sizeof(double) * (size_t)m * wy_stride(ka));
     g->br1.ensure(sizeof(double) * (size_t)ka * ka);
     g->br2.ensure(sizeof(double) * (size_t)ka * ka);
     g->br.ensure(sizeof(double) * (size_t)ka * ka);
@@ -1037,16 +1038,15 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                                          cudaMemcpyDeviceToDevice, s));
                 // least squares: the Householder QR of block column j and every column's residual
                 if (ka <= 64) {
+                    double* wy = g->bwy.as<double>();  // each block column's compact-WY form (V, T^T)
                     if (j > 0) {
-                        const int nw = 8;
-                        const size_t sm = sizeof(double) * (2 * (2 * (size_t)ka * ka + ka) + (size_t)nw * ka);
+                        const size_t sm = apply_prev_smem(ka);
                         ensure_smem_limit((const void*)k_bhess_apply_prev, sm);
-                        k_bhess_apply_prev<<<(ka + nw - 1) / nw, 32 * nw, sm, s>>>(H, (int)L, g->btau.as<double>(),
-                                                                                   ka, j);
+                        k_bhess_apply_prev<<<(ka + kApplyCols - 1) / kApplyCols, 256, sm, s>>>(H, (int)L, wy, ka, j);
                         BIE_CK(cudaGetLastError());
                     }
                     k_bhess_qr_tile<<<1, 512, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
-                                                      g->bres.as<double>());
+                                                      g->bres.as<double>(), wy + (size_t)j * wy_stride(ka));
                 } else {
                     k_bhess_qr_step<<<1, 256, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
                                                       g->bres.as<double>());
@@ -1216,7 +1216,7 @@ void geom_trim(bie_geom* g) {
                       &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid, &g->dpart, &g->rr,
                       &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol, &g->srcpack, &g->glist, &g->bv, &g->bq,
                       &g->bvj, &g->bh, &g->bgv, &g->btau, &g->br1, &g->br2, &g->br, &g->bh2, &g->bres, &g->bidx,
-                      &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp};
+                      &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp, &g->bwy};
     for (auto* b : ws) b->release();
     for (auto& c : g->gcache) {
         for (auto ex : c.exec)
@@ -1272,7 +1272,7 @@ void geom_destroy(bie_geom* g) {
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
                            &g->dpart, &g->rr, &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol, &g->srcpack, &g->glist,
                            &g->bv, &g->bq, &g->bvj, &g->bh, &g->bgv, &g->btau, &g->br1, &g->br2, &g->br, &g->bh2,
-                           &g->bres, &g->bidx, &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp};
+                           &g->bres, &g->bidx, &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp, &g->bwy};
         for (auto* b : all) b->release();
         if (g->blas) cublasDestroy(g->blas);
         for (auto& r : g->prof_pending) {

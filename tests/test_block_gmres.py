@@ -67,7 +67,7 @@ def test_block_wide_block_vs_per_column(bie, small):
 def test_block_equals_looped(bie, small):
     """The reference's check (test/solver/multi_rhs.jl:59-66): block == column by column."""
     itf, op, src, X = small
-    S_block, _ = bie.solve_dielectric_box3d_block(itf, src, 4.0, rtol=1e-10, block=True)
+    S_block, _ = bie.solve_dielectric_box3d_block(itf, src, 4.0, rtol=1e-10)  # block GMRES is the default
     S_loop = np.stack([bie.solve_dielectric_box3d_block(itf, [s_], 4.0, rtol=1e-10)[0][:, 0] for s_ in src], axis=1)
     assert np.all(rel_cols(S_block, S_loop) < 1e-6)
 

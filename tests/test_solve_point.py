@@ -33,5 +33,10 @@ def test_solve_point_equals_rhs_then_solve(bie, k, precision):
     S2, st2 = bie.gpu_solve_sources(op, srcs, 4.0, rtol=1e-11, precision=precision)
     assert st1.solved and st2.solved and st1.iterations == st2.iterations
     assert np.array_equal(S1, S2)
+    # the block API (block GMRES by default, as Krylov.block_gmres) is the same call
     S3, _ = bie.solve_dielectric_box3d_block(itf, srcs, 4.0, rtol=1e-11, precision=precision, precondition=False)
-    assert np.array_equal(S3, S2)
+    S4, _ = bie.gpu_solve_sources(op, srcs, 4.0, rtol=1e-11, precision=precision, block=True)
+    assert np.array_equal(S3, S4)
+    S5, _ = bie.solve_dielectric_box3d_block(itf, srcs, 4.0, rtol=1e-11, precision=precision, precondition=False,
+                                             block=False)
+    assert np.array_equal(S5, S2)
