@@ -147,6 +147,8 @@ struct Prof {
             BIE_CK(cudaEventRecord(a, s));
         }
     }
+    // further launches of this kind inside the scope (several kernels under one scope)
+    void add(int n) { g->acc[kind].launches += n; }
     ~Prof() {
         if (!a) return;
         cudaEvent_t b = nullptr;
@@ -874,9 +876,9 @@ void gram(bie_geom* g, cublasHandle_t h, const double* Q, int ka, int64_t n, dou
 // for the reduced-precision inner solves that stop near 1e-6): Q_old = R^T Q_new, R = R2 R1
 // (ka x ka upper) into Rout (ld ldr). Up to 64 columns the Gram matrix comes from chunked
 // DGEMMs, is factored and inverted in shared memory and applied as a DGEMM with R^-T; wider
-// blocks use SYRK and TRSM.
-void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double* Rout, int ldr, cudaStream_t s,
-             int passes = 2) {
+// blocks use SYRK and TRSM. Returns the number of this library's kernels it launched.
+int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double* Rout, int ldr, cudaStream_t s,
+            int passes = 2) {
     const double one = 1.0, zero = 0.0;
     double* R1 = g->br1.as<double>();
     double* R2 = g->br2.as<double>();
@@ -909,13 +911,15 @@ void cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double
                     "trsm");
         }
     }
+    const int per_pass = ka <= 64 ? 2 : 1;  // k_sum_partials + k_chol_inv_smem, or k_chol_upper
     if (passes == 1) {
         BIE_CK(cudaMemcpy2DAsync(Rout, sizeof(double) * (size_t)ldr, R1, sizeof(double) * (size_t)ka,
                                  sizeof(double) * (size_t)ka, (size_t)ka, cudaMemcpyDeviceToDevice, s));
-        return;
+        return per_pass;
     }
     k_trmm_upper<<<grid1((int64_t)ka * ka), 256, 0, s>>>(R2, ka, R1, ka, Rout, ldr, ka);
     BIE_CK(cudaGetLastError());
+    return passes * per_pass + 1;
 }
 
 // Block GMRES (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285): the active
@@ -986,11 +990,15 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
     bool first = true, conv = false;
     while (true) {
         // residual of the cycle: the right-hand side, or the true residual of the iterate
-        k_gather_cols<<<grid1(nka), 256, 0, s>>>(dr, k, g->bidx.as<int>(), ka, n, Ra);
-        BIE_CK(cudaGetLastError());
+        {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            k_gather_cols<<<grid1(nka), 256, 0, s>>>(dr, k, g->bidx.as<int>(), ka, n, Ra);
+            BIE_CK(cudaGetLastError());
+        }
         if (!first) {
             apply_op(g, Xa, Q, ka, prec, flags, nullptr, s);
             ++res.matvecs;
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
             k_axpby<<<grid1(nka), 256, 0, s>>>(-1.0, Q, 1.0, Ra, n, ka, nullptr);
             BIE_CK(cudaGetLastError());
         }
@@ -999,8 +1007,8 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         BIE_CK(cudaMemsetAsync(Gv, 0, sizeof(double) * (size_t)L * ka, s));
         // V_0 S_0 = R (Cholesky QR); Gv = [S_0; 0]
         {
-            Prof pf(g, BIE_KERNEL_KRYLOV, s);
-            cholqr2(g, h, Ra, ka, n, Gv, (int)L, s, one_pass ? 1 : 2);
+            Prof pf(g, BIE_KERNEL_KRYLOV, s, 0);
+            pf.add(cholqr2(g, h, Ra, ka, n, Gv, (int)L, s, one_pass ? 1 : 2));
             BIE_CK(cudaMemcpy2DAsync(M, pitchL, Ra, pitchK, pitchK, (size_t)n, cudaMemcpyDeviceToDevice, s));
         }
         int jend = 0;
@@ -1011,7 +1019,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
             apply_op(g, Vj, Q, ka, prec, flags, pre, s);  // W = A (p .* V_j), held as Q = W^T
             ++res.matvecs;
             {
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                Prof pf(g, BIE_KERNEL_KRYLOV, s, 0);
                 double* Hc = H + (size_t)j * ka * L;  // block column j
                 // classical Gram-Schmidt: H = V^T W and W -= V H, i.e. H = M_j Q^T, Q -= H^T M_j
                 blas_ck(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)rows, ka, (int)n, &one, M, (int)L, Q, ka, &zero,
@@ -1033,7 +1041,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                             "geam");
                 }
                 // the new block: W = V_{j+1} R, R into H's block (j + 1, j)
-                cholqr2(g, h, Q, ka, n, Hc + rows, (int)L, s, one_pass ? 1 : 2);
+                pf.add(cholqr2(g, h, Q, ka, n, Hc + rows, (int)L, s, one_pass ? 1 : 2));
                 BIE_CK(cudaMemcpy2DAsync(M + (size_t)(j + 1) * ka, pitchL, Q, pitchK, pitchK, (size_t)n,
                                          cudaMemcpyDeviceToDevice, s));
                 // least squares: the Householder QR of block column j and every column's residual
@@ -1044,10 +1052,13 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                         ensure_smem_limit((const void*)k_bhess_apply_prev, sm);
                         k_bhess_apply_prev<<<(ka + kApplyCols - 1) / kApplyCols, 256, sm, s>>>(H, (int)L, wy, ka, j);
                         BIE_CK(cudaGetLastError());
+                        pf.add(1);
                     }
+                    pf.add(1);
                     k_bhess_qr_tile<<<1, 512, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
                                                       g->bres.as<double>(), wy + (size_t)j * wy_stride(ka));
                 } else {
+                    pf.add(1);
                     k_bhess_qr_step<<<1, 256, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
                                                       g->bres.as<double>());
                 }
@@ -1065,7 +1076,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         }
         // Y = R^-1 Gv[0 : jend ka], x += p .* (V Y)
         {
-            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);  // k_add_rows_scaled (TRSM and DGEMM are cuBLAS's)
             const int rows = jend * ka;
             blas_ck(cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, ka,
                                 &one, H, (int)L, Gv, (int)L),
@@ -1079,8 +1090,11 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         if (conv || it >= itmax) break;
         first = false;
     }
-    k_scatter_cols<<<grid1(nka), 256, 0, s>>>(Xa, ka, g->bidx.as<int>(), k, n, dx);
-    BIE_CK(cudaGetLastError());
+    {
+        Prof pf(g, BIE_KERNEL_KRYLOV, s);
+        k_scatter_cols<<<grid1(nka), 256, 0, s>>>(Xa, ka, g->bidx.as<int>(), k, n, dx);
+        BIE_CK(cudaGetLastError());
+    }
     for (int a = 0; a < ka; ++a) res.col_iters[idx[a]] = it;
     res.iters = it;
     res.all_converged = conv;
