@@ -454,14 +454,21 @@ class GeometryCache:
             itf = self.bie.single_dielectric_box3d(*sides, nq, self.lec[key], eps_in, 1.0)
         else:
             itf = box_for_nodes(self.bie, sides, nq, eps_in, target)
+        # room for this geometry's blocks, reserved before the build so that concurrent builders
+        # do not all claim the same free budget (the set-up's transient device memory included)
+        reserve = int(1.25 * self.live_estimate(itf))
         with self.lock:
-            # room for this geometry's blocks (estimated from the first build's size when known)
-            self._evict_for(self.live_estimate(itf))
-        op = self.bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, self.wl["up_tol"], self.wl["max_order"],
-                                                           device=self.device, keep_host_blocks=False,
-                                                           nthreads=self.nthreads)
-        n, nb, b = C.c_int64(), C.c_int64(), C.c_size_t()
-        _abi.check(_abi.lib().bie_geom_info(op.geom._h, C.byref(n), C.byref(nb), C.byref(b)))
+            self._evict_for(reserve)
+            self.used += reserve
+        try:
+            op = self.bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, self.wl["up_tol"], self.wl["max_order"],
+                                                               device=self.device, keep_host_blocks=False,
+                                                               nthreads=self.nthreads)
+            n, nb, b = C.c_int64(), C.c_int64(), C.c_size_t()
+            _abi.check(_abi.lib().bie_geom_info(op.geom._h, C.byref(n), C.byref(nb), C.byref(b)))
+        finally:
+            with self.lock:
+                self.used -= reserve
         dt = time.perf_counter() - t1
         with self.lock:
             rebuild = key in self.lec

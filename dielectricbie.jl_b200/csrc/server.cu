@@ -17,9 +17,12 @@
 // idle geometries do not take memory that admission counts on. A batch whose device
 // allocation fails anyway releases its own workspace and runs once more when every batch in
 // flight is such a retry; retries run one at a time, and no new batch is admitted while one
-// waits, so two batches that fail together do not wait for each other. Every column of a block solve runs its own Krylov process,
-// so a request's result does not depend on what it was batched with beyond
-// floating-point rounding.
+// waits, so two batches that fail together do not wait for each other. A retry that fails
+// again (memory held outside the server) backs off and tries again a bounded number of
+// times. With the default solve options every column of a block solve runs its own Krylov
+// process, so a request's result does not depend on what it was batched with beyond
+// floating-point rounding; requests that ask for block GMRES share one Krylov space with
+// their batch-mates and agree with a solo solve within the tolerance.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -105,6 +108,10 @@ namespace {
 // not fill the GPU and per-iteration fixed costs dominate; a larger geometry runs alone.
 constexpr int64_t kGroupMaxNodes = 24576;
 
+// Attempts of a batch whose device allocation failed (the first run included); the waits
+// between the later ones are 0.25, 0.5, 1, 2 s.
+constexpr int kEnomemAttempts = 6;
+
 // Whether a batch led by request r can join a group solve.
 bool groupable(const Request& r) {
     return r.point && (r.o.precision == BIE_BF16X3 || r.o.precision == BIE_BF16X6) && !r.o.precondition &&
@@ -174,6 +181,10 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
     st.col_iterations = col_it.data();
     st.col_resid = col_res.data();
     auto solve = [&]() {
+        int inj = s->inject_enomem.load();
+        while (inj > 0 && !s->inject_enomem.compare_exchange_weak(inj, inj - 1)) {
+        }
+        if (inj > 0) throw Error(BIE_ENOMEM, "injected allocation failure (test hook)");
         return point ? solve_point_host(r0->g, src.data(), q.data(), eps.data(), K, S.data(), r0->o, &st)
                      : solve_host(r0->g, F.data(), S.data(), K, r0->o, &st);
     };
@@ -182,10 +193,6 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
     const auto t_start = Clock::now();
     try {
         try {
-            int inj = s->inject_enomem.load();
-            while (inj > 0 && !s->inject_enomem.compare_exchange_weak(inj, inj - 1)) {
-            }
-            if (inj > 0) throw Error(BIE_ENOMEM, "injected allocation failure (test hook)");
             rc = solve();
         } catch (const Error& e) {
             if (e.code != BIE_ENOMEM) throw;
@@ -212,15 +219,31 @@ void run_batch(bie_server* s, std::vector<std::shared_ptr<Request>>& batch) {
             } waiting(s);
             s->cv_done.notify_all();  // a retry already waiting may now see only retries in flight
             std::lock_guard<std::mutex> turn(s->retry_mu);
-            {
-                std::unique_lock<std::mutex> lk(s->mu);
-                s->cv_done.wait_for(lk, std::chrono::seconds(300),
-                                    [&] { return s->inflight <= s->retry_waiters || s->stop; });
+            // Memory held outside the server (the caller's other threads building geometries,
+            // other libraries) is released on its own schedule: a retry that meets ENOMEM again
+            // backs off (0.25 s, doubling) and tries again, up to kEnomemAttempts runs in all.
+            for (int attempt = 1;; ++attempt) {
+                {
+                    std::unique_lock<std::mutex> lk(s->mu);
+                    s->cv_done.wait_for(lk, std::chrono::seconds(300),
+                                        [&] { return s->inflight <= s->retry_waiters || s->stop; });
+                }
+                st = bie_stats{};
+                st.col_iterations = col_it.data();
+                st.col_resid = col_res.data();
+                try {
+                    rc = solve();
+                    break;
+                } catch (const Error& e2) {
+                    if (e2.code != BIE_ENOMEM || attempt >= kEnomemAttempts - 1 || s->stop) throw;
+                }
+                geom_trim(r0->g);
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    s->cnt.enomem_retries += 1;
+                }
+                std::this_thread::sleep_for(std::chrono::milliseconds(250 << (attempt - 1)));
             }
-            st = bie_stats{};
-            st.col_iterations = col_it.data();
-            st.col_resid = col_res.data();
-            rc = solve();
         }
         if (rc != BIE_OK) err = "solver did not converge to the requested tolerance";
     } catch (const Error& e) {

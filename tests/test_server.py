@@ -124,6 +124,34 @@ def test_server_concurrent_enomem_retries_complete_promptly(bie, stream, monkeyp
         assert st.solved and np.all(rel_cols(S, ref) < TOL)
 
 
+def test_server_enomem_retry_backs_off(bie, stream, monkeypatch):
+    """A batch whose retry meets ENOMEM again (memory held outside the server) backs off
+    (0.25 s, 0.5 s, ...) and runs again, six runs in all: three injected failures in a row
+    still complete with sigma as alone; ten give up with BIE_ENOMEM after six runs."""
+    import time
+    from dielectricbie_jl_b200 import _abi
+    ops, reqs = stream
+    gi, F = reqs[0]
+    ref = bie.gpu_solve(ops[gi][1], F, rtol=1e-10, precision="bf16x3")[0]
+    monkeypatch.setenv("BIE_TEST_SERVER_ENOMEM", "3")
+    t0 = time.perf_counter()
+    with bie.SolveServer(max_slots=1, max_batch_rhs=64) as srv:
+        S, st, _ = srv.result(srv.submit(ops[gi][1], F, rtol=1e-10, precision="bf16x3"))
+        cnt = srv.counters()
+    elapsed = time.perf_counter() - t0
+    assert st.solved and np.all(rel_cols(S, ref) < TOL)
+    assert cnt["enomem_retries"] == 3 and cnt["completed"] == 1
+    assert 0.7 < elapsed < 60.0, elapsed  # two back-offs: 0.25 s + 0.5 s
+    monkeypatch.setenv("BIE_TEST_SERVER_ENOMEM", "10")
+    with bie.SolveServer(max_slots=1, max_batch_rhs=64) as srv:
+        t = srv.submit(ops[gi][1], F, rtol=1e-10, precision="bf16x3")
+        with pytest.raises(bie.BieError) as ei:
+            srv.result(t)
+        cnt = srv.counters()
+    assert ei.value.code == _abi.BIE_ENOMEM
+    assert cnt["enomem_retries"] == 5  # the first failure and four back-offs: six runs
+
+
 def test_server_point_requests_equal_alone(bie, stream):
     """Point-source requests (bie_server_submit_point: only the sources are queued, the
     right-hand sides are built on the device when the batch runs) merge into block solves and
