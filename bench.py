@@ -45,7 +45,7 @@ WORKLOADS = {
     # serving stream of uneven geometries (sides U[0.5, 2], eps_in log-U[2, 80], n_quad 4 or 6, node
     # counts log-U[n_min, n_max], geometry repeats with p = 0.5, 1-32 point sources per request)
     "cfg4": dict(requests=2000, n_min=2000, n_max=200000, repeat=0.5, rate=20.0, seed=4, rtol=1e-8,
-                 up_tol=1e-9, max_order=8, k=0, restart=60, resident_fraction=0.5, builders=4),
+                 up_tol=1e-9, max_order=8, k=0, restart=60, resident_fraction=0.45, builders=2),
 }
 
 # lattice of 4 x 4 x 2 cubes (side 0.5, gap 0.2), 16 sources at cell-corner centres between cubes
@@ -447,6 +447,7 @@ class GeometryCache:
 
     def _build(self, key, spec):
         import ctypes as C
+        import torch
         from dielectricbie_jl_b200 import _abi
         sides, nq, eps_in, target = spec
         t1 = time.perf_counter()
@@ -460,6 +461,15 @@ class GeometryCache:
         with self.lock:
             self._evict_for(reserve)
             self.used += reserve
+        # and room on the device beside the solves in flight: a build waits (at most 60 s) until
+        # its reservation and a margin are free, so that it does not take the memory of batches
+        # the server has admitted
+        t_gate = time.perf_counter()
+        while time.perf_counter() - t_gate < 60.0:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            if free >= reserve + (8 << 30):
+                break
+            time.sleep(0.05)
         try:
             op = self.bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, self.wl["up_tol"], self.wl["max_order"],
                                                                device=self.device, keep_host_blocks=False,

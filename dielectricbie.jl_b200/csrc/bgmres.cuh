@@ -61,14 +61,19 @@ __global__ void k_chol_upper(double* __restrict__ G, int k, int ldg, int* __rest
     }
 }
 
+constexpr int kCholThreads = 1024;  // block size of k_chol_inv_smem in the solver
+
 // Cholesky factor R of the k x k Gram matrix G (ld k, upper triangle read) and its inverse,
 // in shared memory (2 k (k + 1) doubles, k <= 64): R into Rout (ld ldr, lower triangle zeroed),
 // R^-1 into Rinv (ld k). Pivots are clamped as in k_chol_upper. The factorisation is
 // right-looking with one barrier per pivot (row p of the factor goes to its own array while
-// the trailing matrix is updated from the unscaled row); the inverse is formed column by
-// column, one warp per column, by back substitution with the column in registers.
-__global__ void __launch_bounds__(1024) k_chol_inv_smem(const double* __restrict__ G, int k, double* __restrict__ Rout,
-                                                        int ldr, double* __restrict__ Rinv, int* __restrict__ nclamp) {
+// the trailing matrix is updated from the unscaled row; thread (q, rg) updates row q = tid
+// mod 64 in the columns r = rg mod (blockDim.x / 64)). The inverse is formed by back
+// substitution, warp w taking columns w + m nwarp with the columns in registers and each
+// column of R read once for all of them. NT (the block size): 256, 512 or 1024.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_chol_inv_smem(const double* __restrict__ G, int k, double* __restrict__ Rout,
+                                                      int ldr, double* __restrict__ Rinv, int* __restrict__ nclamp) {
     extern __shared__ double sm[];
     const int ld = k + 1;     // padded: a row of the matrix spreads over the shared-memory banks
     double* A = sm;           // k x k, ld: the trailing matrix
@@ -90,8 +95,7 @@ __global__ void __launch_bounds__(1024) k_chol_inv_smem(const double* __restrict
     }
     __syncthreads();
     const double fl = s_floor;
-    // thread (q, rg): row q = tid mod 64 of the trailing matrix, columns r = rg + 16 m
-    const int qq = tid & 63, rg = tid >> 6;
+    const int qq = tid & 63, rg = tid >> 6, ng = blockDim.x >> 6;  // ng: a power of two
     for (int p = 0; p < k; ++p) {
         double d = A[p + p * ld];
         const bool clamp = !(d > fl);
@@ -101,8 +105,8 @@ __global__ void __launch_bounds__(1024) k_chol_inv_smem(const double* __restrict
         // step p reads row p and writes rows > p of A and row p of R: one barrier per pivot
         if (qq > p && qq < k) {
             const double apq = A[p + qq * ld] * inv;
-            const int r0 = p + 1 + ((rg - (p + 1)) & 15);  // first r >= p + 1 with r = rg mod 16
-            for (int r = r0; r < k; r += 16)
+            const int r0 = p + 1 + ((rg - (p + 1)) & (ng - 1));  // first r >= p + 1 with r = rg mod ng
+            for (int r = r0; r < k; r += ng)
                 if (r >= qq) A[qq + r * ld] -= apq * (A[p + r * ld] * inv);
         }
         if (tid >= p && tid < k) R[p + tid * ld] = tid == p ? piv : A[p + tid * ld] * inv;
@@ -112,20 +116,39 @@ __global__ void __launch_bounds__(1024) k_chol_inv_smem(const double* __restrict
     for (int i = tid; i < k; i += blockDim.x) s_rinv[i] = 1.0 / R[i + i * ld];
     __syncthreads();
     // column jj of R^-1: x = e_jj; for l = jj .. 0: x_l /= R_ll, x_i -= R_il x_l (i < l);
-    // lane holds rows lane and lane + 32
-    for (int jj = warp; jj < k; jj += nwarp) {
-        double x0 = lane == jj ? 1.0 : 0.0, x1 = lane + 32 == jj ? 1.0 : 0.0;
-        for (int l = jj; l >= 0; --l) {
-            const double xl = __shfl_sync(0xFFFFFFFFu, l < 32 ? x0 : x1, l & 31) * s_rinv[l];
+    // lane holds rows lane and lane + 32 of up to 8 columns jj = warp + m nwarp
+    constexpr int MC = 2048 / NT;  // columns per warp: 64 / (NT / 32)
+    double x0[MC], x1[MC];
+    int top = -1;
+#pragma unroll
+    for (int m = 0; m < MC; ++m) {
+        const int jj = warp + m * nwarp;
+        x0[m] = lane == jj ? 1.0 : 0.0;
+        x1[m] = lane + 32 == jj ? 1.0 : 0.0;
+        if (jj < k) top = jj;
+    }
+    for (int l = top; l >= 0; --l) {
+        const double rl = s_rinv[l];
+        const double u0 = lane < l ? R[lane + l * ld] : 0.0;
+        const double u1 = lane + 32 < l ? R[lane + 32 + l * ld] : 0.0;
+#pragma unroll
+        for (int m = 0; m < MC; ++m) {
+            if (warp + m * nwarp >= k) continue;  // uniform per warp
+            const double xl = __shfl_sync(0xFFFFFFFFu, l < 32 ? x0[m] : x1[m], l & 31) * rl;
             if (lane == (l & 31)) {
-                if (l < 32) x0 = xl;
-                else x1 = xl;
+                if (l < 32) x0[m] = xl;
+                else x1[m] = xl;
             }
-            if (lane < l) x0 -= R[lane + l * ld] * xl;
-            if (lane + 32 < l) x1 -= R[lane + 32 + l * ld] * xl;
+            x0[m] = fma(-u0, xl, x0[m]);
+            x1[m] = fma(-u1, xl, x1[m]);
         }
-        if (lane < k) Rinv[lane + jj * k] = lane <= jj ? x0 : 0.0;
-        if (lane + 32 < k) Rinv[lane + 32 + jj * k] = lane + 32 <= jj ? x1 : 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < MC; ++m) {
+        const int jj = warp + m * nwarp;
+        if (jj >= k) continue;
+        if (lane < k) Rinv[lane + jj * k] = lane <= jj ? x0[m] : 0.0;
+        if (lane + 32 < k) Rinv[lane + 32 + jj * k] = lane + 32 <= jj ? x1[m] : 0.0;
     }
     for (int e = tid; e < k * k; e += blockDim.x) {
         const int i = e % k, jj = e / k;
@@ -615,6 +638,95 @@ __global__ void __launch_bounds__(256) k_bhess_apply_prev(double* __restrict__ H
                 }
         }
         __syncthreads();  // the window is complete and buffer buf is free for block b + 2
+    }
+}
+
+// k_bhess_apply_q: Z <- Q Z with Q = Q_0 Q_1 .. Q_{jend-1} the product of the block columns'
+// compact-WY reflectors (wy, as written by k_bhess_qr_tile), applied from the last block to the
+// first: on rows b k .. b k + 2k - 1, C <- C - V_b T_b (V_b^T C). Z has (jend + 1) k rows and
+// k columns (ld ldz). With Z = [0; g] (g the last k rows of the transformed right-hand sides)
+// the result is the least-squares residual in the basis, G - H Y, so that the Krylov residual
+// is the basis times Z. Each CTA (256 threads) takes kApplyCols columns and keeps their 2k-row
+// window in shared memory, moving it up by k rows per block; V_b and T_b are read from global
+// memory (one call per Krylov cycle). k <= 64, jend >= 1.
+inline size_t apply_q_smem(int k) {
+    return sizeof(double) * (2 * (size_t)k * k + (size_t)k * (k + 1) + 4 * (size_t)k * kApplyCols);
+}
+__global__ void __launch_bounds__(256) k_bhess_apply_q(const double* __restrict__ wy, int k, int jend,
+                                                       double* __restrict__ Z, int ldz) {
+    constexpr int NC = kApplyCols;
+    extern __shared__ double sm[];
+    const int k2 = 2 * k, bs = wy_stride(k), tid = threadIdx.x, ldt = k + 1;
+    double* V = sm;                 // 2k x k (ld 2k)
+    double* Ts = V + k2 * k;        // k x k (ld k + 1): Ts[a + l ldt] = T[a][l]
+    double* C = Ts + k * ldt;       // 2k x NC (ld 2k)
+    double* W = C + k2 * NC;        // k x NC (ld k)
+    double* W2 = W + k * NC;        // k x NC (ld k)
+    const int q0 = blockIdx.x * NC, nc = min(NC, k - q0);
+    auto colp = [&](int c) { return Z + (int64_t)(q0 + c) * ldz; };
+    {
+        const int r0 = (jend - 1) * k;
+        for (int c = 0; c < NC; ++c)
+            for (int i = tid; i < k2; i += blockDim.x) C[i + c * k2] = c < nc ? colp(c)[r0 + i] : 0.0;
+    }
+    for (int b = jend - 1; b >= 0; --b) {
+        const int r0 = b * k;
+        const double* src = wy + (int64_t)b * bs;
+        for (int e = tid; e < k2 * k; e += blockDim.x) V[e] = src[e];
+        const double* Tt = src + k2 * k;  // Tt[a + l k] = T[l][a]
+        for (int e = tid; e < k * k; e += blockDim.x) {
+            const int a = e / k, l = e - a * k;  // e = l + a k: T[a][l]
+            Ts[a + l * ldt] = Tt[e];
+        }
+        __syncthreads();
+        // W = V^T C: W[t][c] = sum over i = t .. t + k of V[i][t] C[i][c]
+        for (int o = tid; o < k * NC; o += blockDim.x) {
+            const int c = o / k, t = o - c * k;
+            const double* v = V + t * k2 + t;
+            const double* x = C + c * k2 + t;
+            double a0 = 0.0, a1 = 0.0;
+            int i = 0;
+            for (; i + 1 <= k; i += 2) {
+                a0 = fma(v[i], x[i], a0);
+                a1 = fma(v[i + 1], x[i + 1], a1);
+            }
+            if (i == k) a0 = fma(v[i], x[i], a0);
+            W[t + c * k] = a0 + a1;
+        }
+        __syncthreads();
+        // W2 = T W: W2[a][c] = sum over l >= a of T[a][l] W[l][c]
+        for (int o = tid; o < k * NC; o += blockDim.x) {
+            const int c = o / k, a = o - c * k;
+            const double* w = W + c * k;
+            double a0 = 0.0;
+            for (int l = a; l < k; ++l) a0 = fma(Ts[a + l * ldt], w[l], a0);
+            W2[a + c * k] = a0;
+        }
+        __syncthreads();
+        // C -= V W2
+        for (int o = tid; o < k2 * NC; o += blockDim.x) {
+            const int c = o / k2, i = o - c * k2;
+            const int t0 = max(0, i - k), t1 = min(i, k - 1);
+            const double* w = W2 + c * k;
+            double a0 = 0.0;
+            for (int t = t0; t <= t1; ++t) a0 = fma(V[i + t * k2], w[t], a0);
+            C[o] -= a0;
+        }
+        __syncthreads();
+        if (b == 0) {
+            for (int c = 0; c < nc; ++c)
+                for (int i = tid; i < k2; i += blockDim.x) colp(c)[i] = C[i + c * k2];
+        } else {
+            // rows r0 + k .. r0 + 2k - 1 are final; the window moves up by k rows
+            for (int c = 0; c < nc; ++c)
+                for (int i = tid; i < k; i += blockDim.x) {
+                    double* x = C + c * k2;
+                    colp(c)[r0 + k + i] = x[i + k];
+                    x[i + k] = x[i];
+                    x[i] = colp(c)[r0 - k + i];
+                }
+        }
+        __syncthreads();
     }
 }
 

@@ -109,8 +109,8 @@ namespace {
 constexpr int64_t kGroupMaxNodes = 24576;
 
 // Attempts of a batch whose device allocation failed (the first run included); the waits
-// between the later ones are 0.25, 0.5, 1, 2 s.
-constexpr int kEnomemAttempts = 6;
+// between the later ones are 0.25, 0.5, 1, 2, 4, 8 s.
+constexpr int kEnomemAttempts = 8;
 
 // Whether a batch led by request r can join a group solve.
 bool groupable(const Request& r) {

@@ -614,6 +614,7 @@ struct GmresResult {
     int iters = 0;       // iterations (= operator applications inside the Arnoldi loop)
     int matvecs = 0;     // all operator applications incl. restart residuals
     bool all_converged = false;
+    bool resid_written = false;  // bgmres: the residual r - A(p .* u) went to resid_out
     std::vector<int> col_iters;
 };
 
@@ -889,11 +890,11 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
         double* Ri = g->binv.as<double>();
         double* tmp = g->btmp.as<double>();
         const size_t sm = 2 * sizeof(double) * (size_t)ka * (ka + 1);
-        ensure_smem_limit((const void*)k_chol_inv_smem, sm);
+        ensure_smem_limit((const void*)k_chol_inv_smem<kCholThreads>, sm);
         for (int pass = 0; pass < passes; ++pass) {
             double* Rp = pass == 0 ? R1 : R2;
             gram(g, h, Q, ka, n, Gm, s);
-            k_chol_inv_smem<<<1, 1024, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
+            k_chol_inv_smem<kCholThreads><<<1, kCholThreads, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
             BIE_CK(cudaGetLastError());
             blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, ka, &one, Ri, ka, Q, ka, &zero, tmp, ka),
                     "gemm");
@@ -922,6 +923,11 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
     return passes * per_pass + 1;
 }
 
+// The direct-sum operator apply_op runs for (prec, k): 0 FP32, 1 FP64, 2 split-BF16 x3, 3 x6.
+inline int op_kind(int prec, int k) {
+    return use_tc(prec, k) ? (prec == BIE_BF16X6 ? 3 : 2) : (prec == BIE_FP64 ? 1 : 0);
+}
+
 // Block GMRES (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285): the active
 // columns of dr share one block Krylov space. Block Arnoldi with classical Gram-Schmidt
 // against the whole basis (two passes for FP64 solves, one for the reduced-precision inner
@@ -932,9 +938,12 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
 // with the basis are cuBLAS DGEMMs. The basis is kept as the rows of M ((m + 1) ka x n,
 // column-major: node i holds all basis values in a row of M's column i). Solves
 // A(p .* u) = r, x = p .* u into dx (node-major n x k, zero in the inactive columns);
-// m = block iterations per cycle (restart, at most 60).
+// m = block iterations per cycle (restart, at most 60). With resid_out (n x k) and an
+// operator for (resid_prec, k) equal to the one it iterates with, it also writes the solved
+// columns' residual r - A x there (GmresResult::resid_written); resid_out may be dr itself.
 GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
-                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, cudaStream_t s) {
+                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, cudaStream_t s,
+                   double* resid_out = nullptr, int resid_prec = -1) {
     const int64_t n = g->n;
     const bool one_pass = prec != BIE_FP64;
     GmresResult res;
@@ -954,6 +963,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         return res;
     }
     m = std::max(1, std::min({m, itmax, 60}));
+    const bool want_resid = resid_out && ka <= 64 && op_kind(prec, ka) == op_kind(resid_prec, k);
     const int64_t L = (int64_t)(m + 1) * ka;  // rows of the basis and of the Hessenberg matrix
     const int64_t nka = n * ka;
     g->bv.ensure(sizeof(double) * (size_t)L * n);
@@ -1086,6 +1096,30 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                     "gemm");
             k_add_rows_scaled<<<grid1(nka), 256, 0, s>>>(Xa, Q, pre, n, ka);
             BIE_CK(cudaGetLastError());
+        }
+        // The residual of the last cycle from the Arnoldi relation A P V_j = V_{j+1} H_j:
+        // r - A(p .* u) = V (G - H Y) = V Q [0; g], g the last ka rows of the transformed right-hand
+        // sides, Q the block reflectors. It equals an application of the inner operator to the
+        // correction up to FP64 rounding, and replaces it when the caller would update its
+        // residual with that same operator.
+        if ((conv || it >= itmax) && want_resid && jend > 0) {
+            Prof pf(g, BIE_KERNEL_KRYLOV, s, 0);
+            double* Z = g->bh2.as<double>();  // (jend + 1) ka x ka, ld L
+            BIE_CK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)L * ka, s));
+            BIE_CK(cudaMemcpy2DAsync(Z + (size_t)jend * ka, pitchL, Gv + (size_t)jend * ka, pitchL, pitchK, (size_t)ka,
+                                     cudaMemcpyDeviceToDevice, s));
+            const size_t sm = apply_q_smem(ka);
+            ensure_smem_limit((const void*)k_bhess_apply_q, sm);
+            k_bhess_apply_q<<<(ka + kApplyCols - 1) / kApplyCols, 256, sm, s>>>(g->bwy.as<double>(), ka, jend, Z,
+                                                                                (int)L);
+            BIE_CK(cudaGetLastError());
+            blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, (jend + 1) * ka, &one, Z, (int)L, M, (int)L,
+                                &zero, Q, ka),
+                    "gemm");
+            k_scatter_cols<<<grid1(nka), 256, 0, s>>>(Q, ka, g->bidx.as<int>(), k, n, resid_out);
+            BIE_CK(cudaGetLastError());
+            pf.add(2);
+            res.resid_written = true;
         }
         if (conv || it >= itmax) break;
         first = false;
@@ -1546,9 +1580,12 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             // cannot lower the true residual of this pass)
             for (int c = 0; c < k; ++c)
                 eps_in[c] = std::max({o.inner_rtol * rn[c], 0.5 * tol[c], 2.0 * inner_delta * rn[c]});
+            // block GMRES may return the updated residual r - A_low d itself (from its Arnoldi
+            // relation) when A_low is its own operator
             GmresResult r = (o.block && k > 1)
                                 ? bgmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
-                                         o.itmax - iters, o.restart, s)
+                                         o.itmax - iters, o.restart, s, upd_prec != BIE_FP64 ? rbuf : nullptr,
+                                         upd_prec)
                                 : gmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
                                   o.itmax - iters, o.restart, o.check_every, s);
             iters += r.iters;
@@ -1562,11 +1599,13 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             BIE_CK(cudaGetLastError());
             ++outer;
             if (upd_prec != BIE_FP64) {
-                // r -= A_low d  (d = 0 in the frozen columns)
-                apply_op(g, g->dd.as<double>(), g->rr.as<double>(), k, upd_prec, o.flags, nullptr, s);
-                ++lpmv;
-                Prof pf(g, BIE_KERNEL_KRYLOV, s);
-                k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, g->rr.as<double>(), 1.0, rbuf, n, k, nullptr);
+                // r -= A_low d  (d = 0 in the frozen columns), unless the block solve returned it
+                if (!r.resid_written) {
+                    apply_op(g, g->dd.as<double>(), g->rr.as<double>(), k, upd_prec, o.flags, nullptr, s);
+                    ++lpmv;
+                    Prof pf(g, BIE_KERNEL_KRYLOV, s);
+                    k_axpby<<<grid1(nk), 256, 0, s>>>(-1.0, g->rr.as<double>(), 1.0, rbuf, n, k, nullptr);
+                }
                 have_true_resid = false;
             } else {
                 // r = F - A64 x

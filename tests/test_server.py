@@ -126,8 +126,8 @@ def test_server_concurrent_enomem_retries_complete_promptly(bie, stream, monkeyp
 
 def test_server_enomem_retry_backs_off(bie, stream, monkeypatch):
     """A batch whose retry meets ENOMEM again (memory held outside the server) backs off
-    (0.25 s, 0.5 s, ...) and runs again, six runs in all: three injected failures in a row
-    still complete with sigma as alone; ten give up with BIE_ENOMEM after six runs."""
+    (0.25 s, 0.5 s, ...) and runs again, eight runs in all: three injected failures in a row
+    still complete with sigma as alone; ten give up with BIE_ENOMEM after eight runs."""
     import time
     from dielectricbie_jl_b200 import _abi
     ops, reqs = stream
@@ -149,7 +149,7 @@ def test_server_enomem_retry_backs_off(bie, stream, monkeypatch):
             srv.result(t)
         cnt = srv.counters()
     assert ei.value.code == _abi.BIE_ENOMEM
-    assert cnt["enomem_retries"] == 5  # the first failure and four back-offs: six runs
+    assert cnt["enomem_retries"] == 7  # the first failure and six back-offs: eight runs
 
 
 def test_server_point_requests_equal_alone(bie, stream):
