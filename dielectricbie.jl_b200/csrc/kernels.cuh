@@ -724,6 +724,40 @@ __global__ void k_backsolve(const double* __restrict__ R, const double* __restri
     for (int i = n; i < m1; ++i) y[i * k + c] = 0.0;
 }
 
+// Coefficients of each column's GMRES residual in its basis: with n = jlast[c] and the
+// rotations G_i of k_givens, r - A u = V (beta e_1 - H y) = V G_0^T .. G_{n-1}^T (gv[n] e_n),
+// formed by undoing the rotations in reverse; z (m1 x k) receives them (zero above n).
+__global__ void k_givens_resid(const double* __restrict__ gv, const double* __restrict__ cs,
+                               const double* __restrict__ sn, const int* __restrict__ jlast, int m1, int k,
+                               double* __restrict__ z) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= k) return;
+    const int n = jlast[c];
+    for (int i = 0; i < m1; ++i) z[i * k + c] = 0.0;
+    z[n * k + c] = gv[n * k + c];
+    for (int i = n - 1; i >= 0; --i) {
+        const double a = z[i * k + c], b = z[(i + 1) * k + c], ci = cs[i * k + c], si = sn[i * k + c];
+        z[i * k + c] = ci * a - si * b;
+        z[(i + 1) * k + c] = si * a + ci * b;
+    }
+}
+
+// out[i][c] = sum over v <= jlast[c] of z[v][c] V_v[i][c] (terms with z = 0 skipped, so a
+// direction left undefined by a breakdown does not enter)
+__global__ void k_basis_combine(double* __restrict__ out, const double* __restrict__ V, int64_t strideV,
+                                const double* __restrict__ z, const int* __restrict__ jlast, int64_t n, int k) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    const int c = (int)(e % k);
+    const int nv = jlast[c] + 1;
+    double s = 0.0;
+    for (int v = 0; v < nv; ++v) {
+        const double zv = z[v * k + c];
+        if (zv != 0.0) s = fma(zv, V[(int64_t)v * strideV + e], s);
+    }
+    out[e] = s;
+}
+
 // X[i][c] += p_i * sum_{v < jlast[c]} y[v][c] V_v[i][c]
 __global__ void k_update_solution(double* __restrict__ X, const double* __restrict__ V, int64_t strideV,
                                   const double* __restrict__ y, const int* __restrict__ jlast, int jmax,

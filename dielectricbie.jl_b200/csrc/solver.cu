@@ -86,6 +86,11 @@ inline bool use_tc(int prec, int k) {
     return (prec == BIE_BF16X3 || prec == BIE_BF16X6) && !(k == 1 || k == 2 || k == 4);
 }
 
+// The direct-sum operator apply_op runs for (prec, k): 0 FP32, 1 FP64, 2 split-BF16 x3, 3 x6.
+inline int op_kind(int prec, int k) {
+    return use_tc(prec, k) ? (prec == BIE_BF16X6 ? 3 : 2) : (prec == BIE_FP64 ? 1 : 0);
+}
+
 namespace {
 
 struct DeviceGuard {
@@ -628,10 +633,13 @@ struct GmresResult {
 // the new direction's norm) serves them and halves the passes over the basis.
 GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, int check_every,
-                  cudaStream_t s) {
+                  cudaStream_t s, double* resid_out = nullptr, int resid_prec = -1) {
     const int64_t n = g->n;
     const int64_t nk = n * (int64_t)k;
     const bool one_pass = prec != BIE_FP64;  // see above
+    // the residual r - A x into resid_out (may be dr) when the caller would form it with this
+    // same operator: from the last cycle's Arnoldi relation, or the cycle-start residual
+    const bool want_resid = resid_out && op_kind(prec, k) == op_kind(resid_prec, k);
     m = std::max(1, std::min(m, itmax));
     const int m1 = m + 1;
     g->V.ensure(sizeof(double) * (size_t)m1 * nk);
@@ -723,11 +731,15 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             act[c] = active0[c] && hb[c] > eps[c] ? 1 : 0;
             nact += act[c];
         }
-        if (nact == 0) {
-            res.all_converged = true;
+        if (nact == 0 || it >= itmax) {
+            res.all_converged = nact == 0;
+            if (want_resid) {  // nothing solved since r was formed
+                if (resid_out != r)
+                    BIE_CK(cudaMemcpyAsync(resid_out, r, sizeof(double) * nk, cudaMemcpyDeviceToDevice, s));
+                res.resid_written = true;
+            }
             break;
         }
-        if (it >= itmax) break;
         upload(g->active, act.data(), k, s);
         BIE_CK(cudaMemsetAsync(g->jlast.p, 0, sizeof(int) * k, s));
         BIE_CK(cudaMemsetAsync(g->gv.p, 0, sizeof(double) * m1 * k, s));
@@ -823,6 +835,16 @@ GmresResult gmres(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
         d2h(act.data(), g->active.p, k, s);
         any = false;
         for (int c = 0; c < k; ++c) any = any || act[c];
+        if ((!any || it >= itmax) && want_resid) {
+            // r - A(p .* u) = V z from the Arnoldi relation A P V_j = V_{j+1} H_j: equal to an
+            // application of the operator to the correction up to FP64 rounding
+            Prof pf(g, BIE_KERNEL_KRYLOV, s, 2);
+            k_givens_resid<<<grid1(k, 64), 64, 0, s>>>(g->gv.as<double>(), g->cs.as<double>(), g->sn.as<double>(),
+                                                       g->jlast.as<int>(), m1, k, g->yv.as<double>());
+            k_basis_combine<<<grid1(nk), 256, 0, s>>>(resid_out, V, nk, g->yv.as<double>(), g->jlast.as<int>(), n, k);
+            BIE_CK(cudaGetLastError());
+            res.resid_written = true;
+        }
         if (!any) {
             res.all_converged = true;
             break;
@@ -921,11 +943,6 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
     k_trmm_upper<<<grid1((int64_t)ka * ka), 256, 0, s>>>(R2, ka, R1, ka, Rout, ldr, ka);
     BIE_CK(cudaGetLastError());
     return passes * per_pass + 1;
-}
-
-// The direct-sum operator apply_op runs for (prec, k): 0 FP32, 1 FP64, 2 split-BF16 x3, 3 x6.
-inline int op_kind(int prec, int k) {
-    return use_tc(prec, k) ? (prec == BIE_BF16X6 ? 3 : 2) : (prec == BIE_FP64 ? 1 : 0);
 }
 
 // Block GMRES (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285): the active
@@ -1580,14 +1597,15 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             // cannot lower the true residual of this pass)
             for (int c = 0; c < k; ++c)
                 eps_in[c] = std::max({o.inner_rtol * rn[c], 0.5 * tol[c], 2.0 * inner_delta * rn[c]});
-            // block GMRES may return the updated residual r - A_low d itself (from its Arnoldi
-            // relation) when A_low is its own operator
+            // GMRES returns the updated residual r - A_low d itself (from its Arnoldi relation)
+            // when A_low is its own operator
             GmresResult r = (o.block && k > 1)
                                 ? bgmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
                                          o.itmax - iters, o.restart, s, upd_prec != BIE_FP64 ? rbuf : nullptr,
                                          upd_prec)
                                 : gmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
-                                  o.itmax - iters, o.restart, o.check_every, s);
+                                        o.itmax - iters, o.restart, o.check_every, s,
+                                        upd_prec != BIE_FP64 ? rbuf : nullptr, upd_prec);
             iters += r.iters;
             lpmv += r.matvecs;
             for (int c = 0; c < k; ++c) col_it[c] += r.col_iters[c];
@@ -1599,7 +1617,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
             BIE_CK(cudaGetLastError());
             ++outer;
             if (upd_prec != BIE_FP64) {
-                // r -= A_low d  (d = 0 in the frozen columns), unless the block solve returned it
+                // r -= A_low d  (d = 0 in the frozen columns), unless GMRES returned it
                 if (!r.resid_written) {
                     apply_op(g, g->dd.as<double>(), g->rr.as<double>(), k, upd_prec, o.flags, nullptr, s);
                     ++lpmv;

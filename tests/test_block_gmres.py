@@ -88,3 +88,20 @@ def test_block_preconditioned_two_materials(bie, orc):
     op = bie.lhs_dielectric_box3d_fmm3d_corrected(itf, 1e-12, 1e-9, 8)
     S, st = bie.gpu_solve(op, B, rtol=1e-14, itmax=600, precision="fp64", precondition=True, block=True)
     assert st.solved and np.all(rel_cols(S, X) < 1e-12), rel_cols(S, X).max()
+
+
+@pytest.mark.parametrize("block", [True, False])
+@pytest.mark.parametrize("restart", [60, 4])
+def test_refined_residual_from_arnoldi_relation(bie, small, block, restart):
+    """The refinement's last residual update comes from the inner GMRES's Arnoldi relation
+    (r - A_low d = V z) instead of an operator application. The FP64 true residual of the
+    result (the solver's own verification) must meet the tolerance within the refinement's
+    bound (the admitted update errs by at most half the tolerance): 8 columns on the
+    tensor-core operator, with and without restarts, block and per-column GMRES."""
+    itf, op, src, X = small
+    rng = np.random.default_rng(31)
+    srcs = [bie.PointSource(tuple(rng.uniform(-0.25, 0.25, 3)), float(rng.standard_normal())) for _ in range(8)]
+    S, st = bie.gpu_solve_sources(op, srcs, 4.0, rtol=1e-10, itmax=400, restart=restart, precision="bf16x3",
+                                  block=block)
+    assert st.solved and st.lowp_matvecs > 0
+    assert st.max_rel_resid <= 1.5e-10, st.max_rel_resid
