@@ -1764,11 +1764,13 @@ struct Member {
     bool converged = false, have_true_resid = true;
     int upd_prec = BIE_FP64;
     // inner GMRES of the current refinement step
-    const double* dr = nullptr;  // right-hand side of the inner solve
+    double* dr = nullptr;        // right-hand side of the inner solve (the outer residual)
     double* dx = nullptr;        // its solution
     std::vector<char> in_act;    // columns the inner solve works on
     bool cycle = false;          // iterates in the current Arnoldi cycle
     bool done = false;           // inner solve finished (all columns converged or itmax)
+    bool want_resid = false;     // the inner solve leaves r - A_low d in dr (its own operator)
+    bool resid_written = false;
     int it = 0;                  // inner iterations
     std::vector<int> gact, jl;
     std::vector<double> hb;
@@ -1890,6 +1892,12 @@ void group_gmres(const std::vector<Member*>& all, int pieces, uint32_t flags, in
             }
             if (nact == 0 || M->it >= itmax) {
                 M->done = true;
+                if (M->want_resid) {  // nothing solved since the cycle's residual was formed
+                    if (!first)
+                        BIE_CK(cudaMemcpyAsync(M->dr, M->g->rr.p,
+                                               sizeof(double) * M->g->n * (size_t)M->k, cudaMemcpyDeviceToDevice, s));
+                    M->resid_written = true;
+                }
                 continue;
             }
             bie_geom* g = M->g;
@@ -1964,7 +1972,21 @@ void group_gmres(const std::vector<Member*>& all, int pieces, uint32_t flags, in
             for (int c = 0; c < M->k; ++c) M->col_it[c] += M->jl[c];
             bool any = false;
             for (int c = 0; c < M->k; ++c) any = any || M->gact[c];
-            if (!any || M->it >= itmax) M->done = true;
+            if (!any || M->it >= itmax) {
+                M->done = true;
+                if (M->want_resid) {
+                    // r - A_low d = V z from the Arnoldi relation (as in gmres), into dr
+                    bie_geom* g = M->g;
+                    const int64_t nk = g->n * (int64_t)M->k;
+                    k_givens_resid<<<grid1(M->k, 64), 64, 0, s>>>(g->gv.as<double>(), g->cs.as<double>(),
+                                                                  g->sn.as<double>(), g->jlast.as<int>(), m1, M->k,
+                                                                  g->yv.as<double>());
+                    k_basis_combine<<<grid1(nk), 256, 0, s>>>(M->dr, g->V.as<double>(), nk,
+                                                              g->yv.as<double>(), g->jlast.as<int>(), g->n, M->k);
+                    BIE_CK(cudaGetLastError());
+                    M->resid_written = true;
+                }
+            }
         }
         first = false;
     }
@@ -2097,6 +2119,8 @@ int solve_group(bie_geom* const* gs, int G, const double* const* dF, double* con
             M->in_act = M->act;
             M->dr = M->g->xo.as<double>();
             M->dx = M->g->dd.as<double>();
+            M->want_resid = (M->upd_prec == BIE_BF16X3 && pieces == 2) || (M->upd_prec == BIE_BF16X6 && pieces == 3);
+            M->resid_written = false;
             act.push_back(M);
         }
         if (act.empty()) break;
@@ -2116,7 +2140,10 @@ int solve_group(bie_geom* const* gs, int G, const double* const* dF, double* con
             BIE_CK(cudaGetLastError());
             M->outer += 1;
             if (M->upd_prec != BIE_FP64) {
-                low[M->upd_prec].push_back(M);
+                if (M->resid_written)
+                    M->have_true_resid = false;  // the inner solve left r - A_low d in xo
+                else
+                    low[M->upd_prec].push_back(M);
             } else {
                 apply_op(g, M->dX, g->xo.as<double>(), k, BIE_FP64, o.flags, nullptr, s);
                 M->f64mv += 1;
