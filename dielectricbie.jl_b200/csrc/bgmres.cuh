@@ -2,7 +2,10 @@
 // the k x k Gram matrices (CholQR of each new block of basis vectors) and their inverses,
 // their products, the incremental Householder QR of the block upper-Hessenberg matrix with
 // its right-hand sides, partial-sum reduction and column gathers. One CTA runs each
-// factorisation step; blocks of up to 64 columns keep their tiles in shared memory.
+// factorisation step (a Cholesky, a new block's reflectors); for blocks of up to 64 columns
+// each block column's reflectors are also kept in compact-WY form, which several CTAs apply
+// as small matrix products (the earlier blocks to a new block column, and all blocks in
+// reverse to form the Krylov residual).
 //
 // Storage is column-major: A[i + j * lda].
 #pragma once
