@@ -21,54 +21,14 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// In-place Cholesky factor of the symmetric positive (semi)definite k x k matrix G
-// (upper triangle read): G = R^T R with R upper triangular written to the upper triangle,
-// the strict lower triangle zeroed. A pivot below 1e-30 max(diag G) (a direction the block
-// cannot extend: its columns are linearly dependent to working precision) is replaced by
-// that floor and counted in *nclamp, so the basis stays orthonormal and the corresponding
-// coupling in the Hessenberg matrix is tiny. Used for blocks wider than 64 columns.
-__global__ void k_chol_upper(double* __restrict__ G, int k, int ldg, int* __restrict__ nclamp) {
-    __shared__ double s_piv, s_floor;
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        double mx = 0.0;
-        for (int i = 0; i < k; ++i) mx = fmax(mx, G[i + (int64_t)i * ldg]);
-        s_floor = mx > 0.0 ? 1e-30 * mx : 1e-300;
-    }
-    __syncthreads();
-    for (int p = 0; p < k; ++p) {
-        if (tid == 0) {
-            double d = G[p + (int64_t)p * ldg];
-            if (!(d > s_floor)) {
-                d = s_floor;
-                if (nclamp) atomicAdd(nclamp, 1);
-            }
-            s_piv = sqrt(d);
-            G[p + (int64_t)p * ldg] = s_piv;
-        }
-        __syncthreads();
-        const double piv = s_piv;
-        for (int q = p + 1 + tid; q < k; q += blockDim.x) G[p + (int64_t)q * ldg] /= piv;
-        __syncthreads();
-        const int w = k - p - 1;
-        const int64_t cnt = (int64_t)w * w;
-        for (int64_t e = tid; e < cnt; e += blockDim.x) {
-            const int q = p + 1 + (int)(e / w), r = p + 1 + (int)(e % w);
-            if (q <= r) G[q + (int64_t)r * ldg] -= G[p + (int64_t)q * ldg] * G[p + (int64_t)r * ldg];
-        }
-        __syncthreads();
-    }
-    for (int64_t e = tid; e < (int64_t)k * k; e += blockDim.x) {
-        const int i = (int)(e % k), j = (int)(e / k);
-        if (i > j) G[i + (int64_t)j * ldg] = 0.0;
-    }
-}
-
 constexpr int kCholThreads = 1024;  // block size of k_chol_inv_smem in the solver
 
 // Cholesky factor R of the k x k Gram matrix G (ld k, upper triangle read) and its inverse,
 // in shared memory (2 k (k + 1) doubles, k <= 64): R into Rout (ld ldr, lower triangle zeroed),
-// R^-1 into Rinv (ld k). Pivots are clamped as in k_chol_upper. The factorisation is
+// R^-1 into Rinv (ld k). A pivot below 1e-30 max(diag G) (a direction the block cannot
+// extend: its columns are linearly dependent to working precision) is replaced by that floor
+// and counted in *nclamp, so the basis stays orthonormal and the corresponding coupling in the
+// Hessenberg matrix is tiny. The factorisation is
 // right-looking with one barrier per pivot (row p of the factor goes to its own array while
 // the trailing matrix is updated from the unscaled row; thread (q, rg) updates row q = tid
 // mod 64 in the columns r = rg mod (blockDim.x / 64)). The inverse is formed by back
@@ -225,117 +185,6 @@ __global__ void k_add_rows_scaled(double* __restrict__ X, const double* __restri
 
 namespace bie {
 
-// Applies the reflector (1, v[c + 1 .. c + k]) with scalar tc to column x over rows c .. c + k,
-// the G threads of a group (G consecutive lanes of a warp, sub = lane in the group) sharing the
-// dot product. Every lane of the warp calls it (lanes of an idle group with x = null).
-__device__ __forceinline__ void apply_reflector(const double* __restrict__ v, double tc, double* x, int c, int k,
-                                                int G, int sub) {
-    double part = 0.0;
-    if (x)
-        for (int i = sub; i <= k; i += G) part += (i == 0 ? 1.0 : v[c + i]) * x[c + i];
-    for (int o = G / 2; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
-    const double s = part * tc;
-    if (x)
-        for (int i = sub; i <= k; i += G) x[c + i] -= s * (i == 0 ? 1.0 : v[c + i]);
-}
-
-// Threads per column group: the largest power of two G <= 32 with 2 G k <= blockDim.x (k columns
-// updated at once by blockDim.x / G groups).
-__device__ __forceinline__ int group_width(int k) {
-    int G = 1;
-    while (G < 32 && 2 * G * k <= (int)blockDim.x) G *= 2;
-    return G;
-}
-
-// Forms the Householder reflector of column t0 of the tile (local rows t0 .. t0 + k; LAPACK
-// dlarfg convention: the column becomes (beta, v tail), tau returned) and applies it to the
-// tile's later columns and to the k right-hand-side columns Gt (same rows). Tiles in shared or
-// global memory, ld ldt; red: blockDim.x doubles of shared memory.
-__device__ __forceinline__ double reflect_column(double* T, int ldt, double* Gt, int ldgt, int t0, int k, double* red,
-                                                 double* s_tau, double* s_scale, int G, int sub, int grp, int ngrp) {
-    const int tid = threadIdx.x;
-    double* col = T + (int64_t)t0 * ldt;
-    double part = 0.0;
-    for (int i = 1 + tid; i <= k; i += blockDim.x) part += col[t0 + i] * col[t0 + i];
-    red[tid] = part;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (tid < w) red[tid] += red[tid + w];
-        __syncthreads();
-    }
-    if (tid == 0) {
-        const double sigma = red[0], alpha = col[t0];
-        if (sigma == 0.0) {
-            *s_tau = 0.0;
-            *s_scale = 0.0;
-        } else {
-            const double mu = sqrt(alpha * alpha + sigma);
-            const double beta = alpha <= 0.0 ? mu : -mu;
-            *s_tau = (beta - alpha) / beta;
-            *s_scale = 1.0 / (alpha - beta);
-            col[t0] = beta;
-        }
-    }
-    __syncthreads();
-    const double tc = *s_tau;
-    if (tc != 0.0) {
-        for (int i = 1 + tid; i <= k; i += blockDim.x) col[t0 + i] *= *s_scale;
-        __syncthreads();
-        const int nrest = k - 1 - t0;
-        for (int q0 = 0; q0 < nrest + k; q0 += ngrp) {
-            const int q = q0 + grp;
-            double* x = q < nrest ? T + (int64_t)(t0 + 1 + q) * ldt
-                                  : (q < nrest + k ? Gt + (int64_t)(q - nrest) * ldgt : nullptr);
-            apply_reflector(col, tc, x, t0, k, G, sub);
-        }
-    }
-    __syncthreads();
-    return tc;
-}
-
-// One block column of the incremental Householder QR of the block upper-Hessenberg matrix H
-// ((m + 1) k x m k, ldh = (m + 1) k) with the right-hand sides Gv ((m + 1) k x k, ldg). Block
-// column j (columns jk .. jk + k - 1) holds the new Gram-Schmidt coefficients in rows
-// 0 .. (j + 2) k - 1; its lower k x k block is upper triangular (the CholQR factor), so column
-// c has nonzeros down to row c + k and every reflector spans k + 1 rows. The earlier columns'
-// reflectors (tails below the diagonal, tau) are applied to the block column in order; then
-// each of its columns gets its own reflector, applied to the block's later columns and to Gv.
-// resid[a] = || Gv[(j + 1) k .. (j + 2) k - 1, a] ||, the least-squares residual of
-// right-hand side a. One CTA of 256 threads, everything in global memory (any k).
-__global__ void k_bhess_qr_step(double* __restrict__ H, int ldh, double* __restrict__ tau, double* __restrict__ Gv,
-                                int ldg, int k, int j, double* __restrict__ resid) {
-    __shared__ double red[256];
-    __shared__ double s_tau, s_scale;
-    const int tid = threadIdx.x;
-    const int c0 = j * k;
-    const int G = group_width(k), sub = tid % G, grp = tid / G, ngrp = blockDim.x / G;
-    for (int c = 0; c < c0; ++c) {
-        const double tc = tau[c];
-        if (tc == 0.0) continue;
-        const double* v = H + (int64_t)c * ldh;
-        for (int t0 = 0; t0 < k; t0 += ngrp) {
-            const int t = t0 + grp;
-            apply_reflector(v, tc, t < k ? H + (int64_t)(c0 + t) * ldh : nullptr, c, k, G, sub);
-        }
-    }
-    __syncthreads();
-    // the new block's tile starts at row c0 of column c0: local row t0 == global row c0 + t0
-    double* T = H + (int64_t)c0 * ldh + c0;
-    double* Gt = Gv + c0;
-    for (int t0 = 0; t0 < k; ++t0) {
-        const double tc = reflect_column(T, ldh, Gt, ldg, t0, k, red, &s_tau, &s_scale, G, sub, grp, ngrp);
-        if (tid == 0) tau[c0 + t0] = tc;
-    }
-    for (int a = tid; a < k; a += blockDim.x) {
-        const double* g = Gv + (int64_t)a * ldg;
-        double s = 0.0;
-        for (int i = (j + 1) * k; i < (j + 2) * k; ++i) s += g[i] * g[i];
-        resid[a] = sqrt(s);
-    }
-}
-
-// The two kernels below split k_bhess_qr_step for k <= 64.
-//
 // Sum over the 8 lanes of a column group (lanes 8 c .. 8 c + 7 of a warp).
 __device__ __forceinline__ double group8_sum(double v) {
     v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
@@ -432,7 +281,8 @@ __device__ __forceinline__ void tile_reflector(double (&x)[2][16], int t, int k,
 // sides Gv, and every right-hand side's residual. One CTA of 512 threads: column group
 // G = 4 warp + lane / 8 (8 lanes) holds tile column G and right-hand side G in registers,
 // lane g = lane mod 8 the local rows g + 8 r (r < 16). For reflector t the group of column t
-// forms it (LAPACK dlarfg convention, as reflect_column) and publishes v through shared
+// forms it (LAPACK dlarfg convention: beta = -sign(alpha) mu, tau = (beta - alpha) / beta,
+// tail scaled by 1 / (alpha - beta)) and publishes v through shared
 // memory; after one barrier every group applies it to its columns right of t, over the row
 // slots the reflector meets (tile_reflector; no data-dependent branches).
 //

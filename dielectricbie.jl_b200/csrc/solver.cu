@@ -893,48 +893,34 @@ void gram(bie_geom* g, cublasHandle_t h, const double* Q, int ka, int64_t n, dou
     BIE_CK(cudaGetLastError());
 }
 
-// Orthonormalises the rows of Q (ka x n, column-major, ld ka: the transposed block of ka
+// Orthonormalises the rows of Q (ka x n, column-major, ld ka: the transposed block of ka <= 64
 // vectors) by Cholesky QR applied `passes` times (2: CholQR2, orthogonal to working precision
 // for condition numbers up to about 1e8; 1: orthogonality error about cond^2 1e-16, enough
 // for the reduced-precision inner solves that stop near 1e-6): Q_old = R^T Q_new, R = R2 R1
-// (ka x ka upper) into Rout (ld ldr). Up to 64 columns the Gram matrix comes from chunked
-// DGEMMs, is factored and inverted in shared memory and applied as a DGEMM with R^-T; wider
-// blocks use SYRK and TRSM. Returns the number of this library's kernels it launched.
+// (ka x ka upper) into Rout (ld ldr). The Gram matrix comes from chunked DGEMMs, is factored
+// and inverted in shared memory and applied as a DGEMM with R^-T. Returns the number of this
+// library's kernels it launched.
 int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double* Rout, int ldr, cudaStream_t s,
             int passes = 2) {
     const double one = 1.0, zero = 0.0;
     double* R1 = g->br1.as<double>();
     double* R2 = g->br2.as<double>();
-    if (ka <= 64) {
-        g->binv.ensure(sizeof(double) * (size_t)ka * ka);
-        g->btmp.ensure(sizeof(double) * (size_t)n * ka);
-        double* Gm = g->br.as<double>();
-        double* Ri = g->binv.as<double>();
-        double* tmp = g->btmp.as<double>();
-        const size_t sm = 2 * sizeof(double) * (size_t)ka * (ka + 1);
-        ensure_smem_limit((const void*)k_chol_inv_smem<kCholThreads>, sm);
-        for (int pass = 0; pass < passes; ++pass) {
-            double* Rp = pass == 0 ? R1 : R2;
-            gram(g, h, Q, ka, n, Gm, s);
-            k_chol_inv_smem<kCholThreads><<<1, kCholThreads, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
-            BIE_CK(cudaGetLastError());
-            blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, ka, &one, Ri, ka, Q, ka, &zero, tmp, ka),
-                    "gemm");
-            BIE_CK(cudaMemcpyAsync(Q, tmp, sizeof(double) * (size_t)n * ka, cudaMemcpyDeviceToDevice, s));
-        }
-    } else {
-        for (int pass = 0; pass < passes; ++pass) {
-            double* Rp = pass == 0 ? R1 : R2;
-            blas_ck(cublasDsyrk(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, ka, (int)n, &one, Q, ka, &zero, Rp, ka),
-                    "syrk");
-            k_chol_upper<<<1, 256, 0, s>>>(Rp, ka, ka, g->bflag.as<int>());
-            BIE_CK(cudaGetLastError());
-            blas_ck(cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, ka,
-                                (int)n, &one, Rp, ka, Q, ka),
-                    "trsm");
-        }
+    g->binv.ensure(sizeof(double) * (size_t)ka * ka);
+    g->btmp.ensure(sizeof(double) * (size_t)n * ka);
+    double* Gm = g->br.as<double>();
+    double* Ri = g->binv.as<double>();
+    double* tmp = g->btmp.as<double>();
+    const size_t sm = 2 * sizeof(double) * (size_t)ka * (ka + 1);
+    ensure_smem_limit((const void*)k_chol_inv_smem<kCholThreads>, sm);
+    for (int pass = 0; pass < passes; ++pass) {
+        double* Rp = pass == 0 ? R1 : R2;
+        gram(g, h, Q, ka, n, Gm, s);
+        k_chol_inv_smem<kCholThreads><<<1, kCholThreads, sm, s>>>(Gm, ka, Rp, ka, Ri, g->bflag.as<int>());
+        BIE_CK(cudaGetLastError());
+        blas_ck(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, ka, (int)n, ka, &one, Ri, ka, Q, ka, &zero, tmp, ka), "gemm");
+        BIE_CK(cudaMemcpyAsync(Q, tmp, sizeof(double) * (size_t)n * ka, cudaMemcpyDeviceToDevice, s));
     }
-    const int per_pass = ka <= 64 ? 2 : 1;  // k_sum_partials + k_chol_inv_smem, or k_chol_upper
+    const int per_pass = 2;  // k_sum_partials + k_chol_inv_smem
     if (passes == 1) {
         BIE_CK(cudaMemcpy2DAsync(Rout, sizeof(double) * (size_t)ldr, R1, sizeof(double) * (size_t)ka,
                                  sizeof(double) * (size_t)ka, (size_t)ka, cudaMemcpyDeviceToDevice, s));
@@ -945,42 +931,24 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
     return passes * per_pass + 1;
 }
 
-// Block GMRES (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285): the active
-// columns of dr share one block Krylov space. Block Arnoldi with classical Gram-Schmidt
-// against the whole basis (two passes for FP64 solves, one for the reduced-precision inner
-// solves), each new block orthonormalised by Cholesky QR (twice for FP64 solves, once for
-// the inner solves); the block
-// upper-Hessenberg least-squares problem is updated by Householder reflections one block
-// column per iteration, which gives every column's residual norm. The tall-skinny products
-// with the basis are cuBLAS DGEMMs. The basis is kept as the rows of M ((m + 1) ka x n,
-// column-major: node i holds all basis values in a row of M's column i). Solves
-// A(p .* u) = r, x = p .* u into dx (node-major n x k, zero in the inactive columns);
-// m = block iterations per cycle (restart, at most 60). With resid_out (n x k) and an
-// operator for (resid_prec, k) equal to the one it iterates with, it also writes the solved
-// columns' residual r - A x there (GmresResult::resid_written); resid_out may be dr itself.
-GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
-                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, cudaStream_t s,
-                   double* resid_out = nullptr, int resid_prec = -1) {
+// One block Krylov space (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285) for
+// the columns idx (at most 64) of dr. Block Arnoldi with classical Gram-Schmidt against the
+// whole basis (two passes for FP64 solves, one for the reduced-precision inner solves), each
+// new block orthonormalised by Cholesky QR (twice for FP64 solves, once for the inner
+// solves); the block upper-Hessenberg least-squares problem is updated by Householder
+// reflections one block column per iteration (kept in compact-WY form), which gives every
+// column's residual norm. The tall-skinny products with the basis are cuBLAS DGEMMs. The
+// basis is kept as the rows of M ((m + 1) ka x n, column-major: node i holds all basis values
+// in a row of M's column i). The columns' solution goes to the same columns of dx, their
+// residual r - A x to resid_out when it is not null (from the Arnoldi relation); iterations,
+// operator applications and convergence are merged into res.
+void bgmres_chunk(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
+                  const std::vector<int>& idx, const std::vector<double>& eps, int itmax, int m, cudaStream_t s,
+                  double* resid_out, GmresResult& res) {
     const int64_t n = g->n;
     const bool one_pass = prec != BIE_FP64;
-    GmresResult res;
-    res.col_iters.assign(k, 0);
-    BIE_CK(cudaMemsetAsync(dx, 0, sizeof(double) * n * k, s));
-    // columns that need work: active and above their tolerance
-    g->beta.ensure(sizeof(double) * k);
-    col_norms(g, dr, k, g->beta.as<double>(), s);
-    std::vector<double> nr(k);
-    d2h(nr.data(), g->beta.p, k, s);
-    std::vector<int> idx;
-    for (int c = 0; c < k; ++c)
-        if (active0[c] && nr[c] > eps[c]) idx.push_back(c);
     const int ka = (int)idx.size();
-    if (ka == 0) {
-        res.all_converged = true;
-        return res;
-    }
-    m = std::max(1, std::min({m, itmax, 60}));
-    const bool want_resid = resid_out && ka <= 64 && op_kind(prec, ka) == op_kind(resid_prec, k);
+    const bool want_resid = resid_out != nullptr;
     const int64_t L = (int64_t)(m + 1) * ka;  // rows of the basis and of the Hessenberg matrix
     const int64_t nka = n * ka;
     g->bv.ensure(sizeof(double) * (size_t)L * n);
@@ -989,7 +957,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
     g->bh.ensure(sizeof(double) * (size_t)L * m * ka);
     g->bgv.ensure(sizeof(double) * (size_t)L * ka);
     g->btau.ensure(sizeof(double) * (size_t)m * ka);
-    if (ka <= 64) g->bwy.ensure(sizeof(double) * (size_t)m * wy_stride(ka));
+    g->bwy.ensure(sizeof(double) * (size_t)m * wy_stride(ka));
     g->br1.ensure(sizeof(double) * (size_t)ka * ka);
     g->br2.ensure(sizeof(double) * (size_t)ka * ka);
     g->br.ensure(sizeof(double) * (size_t)ka * ka);
@@ -1072,7 +1040,7 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                 BIE_CK(cudaMemcpy2DAsync(M + (size_t)(j + 1) * ka, pitchL, Q, pitchK, pitchK, (size_t)n,
                                          cudaMemcpyDeviceToDevice, s));
                 // least squares: the Householder QR of block column j and every column's residual
-                if (ka <= 64) {
+                {
                     double* wy = g->bwy.as<double>();  // each block column's compact-WY form (V, T^T)
                     if (j > 0) {
                         const size_t sm = apply_prev_smem(ka);
@@ -1084,10 +1052,6 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
                     pf.add(1);
                     k_bhess_qr_tile<<<1, 512, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
                                                       g->bres.as<double>(), wy + (size_t)j * wy_stride(ka));
-                } else {
-                    pf.add(1);
-                    k_bhess_qr_step<<<1, 256, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
-                                                      g->bres.as<double>());
                 }
                 BIE_CK(cudaGetLastError());
             }
@@ -1119,6 +1083,12 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         // sides, Q the block reflectors. It equals an application of the inner operator to the
         // correction up to FP64 rounding, and replaces it when the caller would update its
         // residual with that same operator.
+        if ((conv || it >= itmax) && want_resid && jend == 0) {
+            // no iteration in this cycle: the residual is the cycle's own
+            Prof pf(g, BIE_KERNEL_KRYLOV, s);
+            k_scatter_cols<<<grid1(nka), 256, 0, s>>>(Ra, ka, g->bidx.as<int>(), k, n, resid_out);
+            BIE_CK(cudaGetLastError());
+        }
         if ((conv || it >= itmax) && want_resid && jend > 0) {
             Prof pf(g, BIE_KERNEL_KRYLOV, s, 0);
             double* Z = g->bh2.as<double>();  // (jend + 1) ka x ka, ld L
@@ -1136,7 +1106,6 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
             k_scatter_cols<<<grid1(nka), 256, 0, s>>>(Q, ka, g->bidx.as<int>(), k, n, resid_out);
             BIE_CK(cudaGetLastError());
             pf.add(2);
-            res.resid_written = true;
         }
         if (conv || it >= itmax) break;
         first = false;
@@ -1147,8 +1116,44 @@ GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, u
         BIE_CK(cudaGetLastError());
     }
     for (int a = 0; a < ka; ++a) res.col_iters[idx[a]] = it;
-    res.iters = it;
-    res.all_converged = conv;
+    res.iters = std::max(res.iters, it);
+    res.all_converged = res.all_converged && conv;
+}
+
+// Block GMRES (the method of Krylov.block_gmres) over the active columns of dr that are above
+// their tolerance, in balanced chunks of at most 64 columns, each its own block Krylov space
+// (the least-squares and CholQR kernels hold up to 64 columns). Solves A(p .* u) = r, x = p .* u
+// into dx (node-major n x k, zero in the other columns); m = block iterations per cycle
+// (restart, at most 60). With resid_out (n x k, may be dr itself) and an operator for
+// (resid_prec, k) equal to the one every chunk iterates with, the solved columns' residual
+// r - A x is written there as well (GmresResult::resid_written).
+GmresResult bgmres(bie_geom* g, const double* dr, double* dx, int k, int prec, uint32_t flags, const double* pre,
+                   const std::vector<double>& eps, const std::vector<char>& active0, int itmax, int m, cudaStream_t s,
+                   double* resid_out = nullptr, int resid_prec = -1) {
+    const int64_t n = g->n;
+    GmresResult res;
+    res.col_iters.assign(k, 0);
+    BIE_CK(cudaMemsetAsync(dx, 0, sizeof(double) * n * k, s));
+    // columns that need work: active and above their tolerance
+    g->beta.ensure(sizeof(double) * k);
+    col_norms(g, dr, k, g->beta.as<double>(), s);
+    std::vector<double> nr(k);
+    d2h(nr.data(), g->beta.p, k, s);
+    std::vector<int> idx;
+    for (int c = 0; c < k; ++c)
+        if (active0[c] && nr[c] > eps[c]) idx.push_back(c);
+    const int ka = (int)idx.size();
+    res.all_converged = true;
+    if (ka == 0) return res;
+    m = std::max(1, std::min({m, itmax, 60}));
+    const int nch = (ka + 63) / 64, csz = (ka + nch - 1) / nch;
+    bool want = resid_out != nullptr;
+    for (int c0 = 0; c0 < ka; c0 += csz) want = want && op_kind(prec, std::min(csz, ka - c0)) == op_kind(resid_prec, k);
+    for (int c0 = 0; c0 < ka; c0 += csz) {
+        const std::vector<int> sub(idx.begin() + c0, idx.begin() + std::min(ka, c0 + csz));
+        bgmres_chunk(g, dr, dx, k, prec, flags, pre, sub, eps, itmax, m, s, want ? resid_out : nullptr, res);
+    }
+    res.resid_written = want;
     return res;
 }
 

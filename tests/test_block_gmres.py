@@ -53,8 +53,9 @@ def test_block_refined_vs_lu(bie, small):
 
 
 def test_block_wide_block_vs_per_column(bie, small):
-    """A block wider than 64 columns (the SYRK/TRSM and global-memory QR path): 80 columns
-    agree with the per-column solve within the refined bar."""
+    """A block wider than 64 columns is solved in balanced chunks of at most 64 (here two block
+    Krylov spaces of 40 columns): 80 columns agree with the per-column solve within the
+    refined bar."""
     itf, op, src, X = small
     rng = np.random.default_rng(21)
     srcs = [bie.PointSource(tuple(rng.uniform(-0.25, 0.25, 3)), float(rng.standard_normal())) for _ in range(80)]
