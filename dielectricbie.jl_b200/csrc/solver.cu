@@ -39,6 +39,8 @@ struct bie_geom {
     // block GMRES workspace: basis, Hessenberg matrix, right-hand sides, small factors
     bie::Buf bv, bq, bvj, bh, bgv, btau, br1, br2, br, bh2, bres, bidx, bflag, xa, ra, binv, bpart, btmp, bwy;
     cublasHandle_t blas = nullptr;  // created on the first block solve
+    double* bres_host = nullptr;    // pinned copy of the block residual norms (64 doubles)
+    cudaEvent_t ev_res = nullptr;   // marks that copy in the stream
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // kernel timing
     struct ProfRec {
@@ -1007,12 +1009,18 @@ void bgmres_chunk(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             BIE_CK(cudaMemcpy2DAsync(M, pitchL, Ra, pitchK, pitchK, (size_t)n, cudaMemcpyDeviceToDevice, s));
         }
         int jend = 0;
+        bool queued = false;  // this iteration's operator application is already in the stream
+        double worst = 0.0;   // max over the columns of residual / tolerance after an iteration
+        auto queue_apply = [&](int jj) {  // W = A (p .* V_jj), held as Q = W^T
+            BIE_CK(cudaMemcpy2DAsync(Vj, pitchK, M + (size_t)jj * ka, pitchL, pitchK, (size_t)n,
+                                     cudaMemcpyDeviceToDevice, s));
+            apply_op(g, Vj, Q, ka, prec, flags, pre, s);
+            ++res.matvecs;
+        };
         for (int j = 0; j < m && it < itmax; ++j) {
             const int64_t rows = (int64_t)(j + 1) * ka;  // basis vectors so far
-            BIE_CK(cudaMemcpy2DAsync(Vj, pitchK, M + (size_t)j * ka, pitchL, pitchK, (size_t)n,
-                                     cudaMemcpyDeviceToDevice, s));
-            apply_op(g, Vj, Q, ka, prec, flags, pre, s);  // W = A (p .* V_j), held as Q = W^T
-            ++res.matvecs;
+            if (!queued) queue_apply(j);
+            queued = false;
             {
                 Prof pf(g, BIE_KERNEL_KRYLOV, s, 0);
                 double* Hc = H + (size_t)j * ka * L;  // block column j
@@ -1057,9 +1065,27 @@ void bgmres_chunk(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
             }
             ++it;
             jend = j + 1;
-            d2h(rsd.data(), g->bres.p, ka, s);
+            // the residual norms to the host. A GMRES iteration lowers a residual by a few times
+            // at most: while the previous one left every column above 16 times its tolerance, the
+            // next iteration will run, and its operator application is queued behind the copy so
+            // that the device works while the host waits for the norms (were the columns to
+            // converge after all, that application is merely unused)
+            if (!g->bres_host) BIE_CK(cudaMallocHost(&g->bres_host, sizeof(double) * 64));
+            if (!g->ev_res) BIE_CK(cudaEventCreateWithFlags(&g->ev_res, cudaEventDisableTiming));
+            BIE_CK(cudaMemcpyAsync(g->bres_host, g->bres.p, sizeof(double) * ka, cudaMemcpyDeviceToHost, s));
+            BIE_CK(cudaEventRecord(g->ev_res, s));
+            if (j > 0 && worst > 16.0 && j + 1 < m && it < itmax) {
+                queue_apply(j + 1);
+                queued = true;
+            }
+            BIE_CK(cudaEventSynchronize(g->ev_res));
             bool all = true;
-            for (int a = 0; a < ka; ++a) all = all && rsd[a] <= epsa[a];
+            worst = 0.0;
+            for (int a = 0; a < ka; ++a) {
+                rsd[a] = g->bres_host[a];
+                all = all && rsd[a] <= epsa[a];
+                worst = std::max(worst, rsd[a] / epsa[a]);
+            }
             if (all) {
                 conv = true;
                 break;
@@ -1345,6 +1371,8 @@ void geom_destroy(bie_geom* g) {
                            &g->bres, &g->bidx, &g->bflag, &g->xa, &g->ra, &g->binv, &g->bpart, &g->btmp, &g->bwy};
         for (auto* b : all) b->release();
         if (g->blas) cublasDestroy(g->blas);
+        if (g->bres_host) cudaFreeHost(g->bres_host);
+        if (g->ev_res) cudaEventDestroy(g->ev_res);
         for (auto& r : g->prof_pending) {
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
