@@ -689,7 +689,8 @@ def gpu_solve(op: GPUDielectricOperator, F, *, rtol: float = 1e-10, atol: float 
               restart: int = 200, precision: Optional[str] = None, inner_rtol: float = 1e-6, max_outer: int = 8,
               precondition: bool = False, check_every: int = 1, raise_on_noconv: bool = False, block: bool = False):
     """Solve A Sigma = F on the device. Returns (Sigma, SolveStats). block=True runs block GMRES
-    (one Krylov space shared by the columns, as Krylov.block_gmres) for more than one column."""
+    (one Krylov space shared by the columns, as Krylov.block_gmres) for 2 to 64 columns; wider
+    blocks run one Arnoldi process per column, which is faster with this library's kernels."""
     Ff, vec = _as_cols(F, op.n)
     k = Ff.shape[1]
     o = _solve_opts(op, rtol, atol, itmax, restart, precision, inner_rtol, max_outer, precondition, check_every,
@@ -865,8 +866,9 @@ def solve_dielectric_box3d_block(interface: DielectricInterface, sources, eps_sr
     """``solve_dielectric_box3d_block`` (src/solver/multi_rhs.jl:270-286) for PointSource right-hand
     sides (the reference takes VolumeSources; the operator is the same). eps_src defaults to each
     panel's eps_in of the first panel (source inside a single box). block=True (the default) solves
-    the columns in one block Krylov space, as the reference's Krylov.block_gmres; block=False runs
-    one Arnoldi process per column. Returns (Sigma, stats)."""
+    up to 64 columns in one block Krylov space, as the reference's Krylov.block_gmres (wider blocks
+    run one Arnoldi process per column, faster here); block=False runs one Arnoldi process per
+    column. Returns (Sigma, stats)."""
     op = batched_lhs_dielectric_box3d_fmm3d_corrected(interface, fmm_tol, up_tol, max_order,
                                                       correct_edges=correct_edges, precision=precision,
                                                       device=device)

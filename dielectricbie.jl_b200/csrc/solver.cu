@@ -933,6 +933,13 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
     return passes * per_pass + 1;
 }
 
+// Whether a solve of k columns runs block GMRES: the option is set and 2 <= k <= 64. Wider
+// blocks run one Arnoldi process per column, which shares one operator application per
+// iteration over all columns; block GMRES in chunks of 64 applies the operator once per chunk
+// (cfg3 box, rtol 1e-10, bf16x3: 96 columns 85-88 ms per column-wise solve against 100-102 ms
+// in chunks, 128 columns 98-99 ms against 104-114 ms).
+inline bool use_block(const bie_solve_opts& o, int k) { return o.block && k > 1 && k <= 64; }
+
 // One block Krylov space (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285) for
 // the columns idx (at most 64) of dr. Block Arnoldi with classical Gram-Schmidt against the
 // whole basis (two passes for FP64 solves, one for the reduced-precision inner solves), each
@@ -1570,7 +1577,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
     g->xo.ensure(sizeof(double) * nk);
     double* rbuf = g->xo.as<double>();  // outer residual F - A x
     if (o.precision == BIE_FP64) {
-        GmresResult r = (o.block && k > 1)
+        GmresResult r = use_block(o, k)
                             ? bgmres(g, dF, dX, k, BIE_FP64, o.flags, pre, tol, act, o.itmax, o.restart, s)
                             : gmres(g, dF, dX, k, BIE_FP64, o.flags, pre, tol, act, o.itmax, o.restart, o.check_every, s);
         iters = r.iters;
@@ -1632,7 +1639,7 @@ int solve_device(bie_geom* g, const double* dF, double* dX, int k, const bie_sol
                 eps_in[c] = std::max({o.inner_rtol * rn[c], 0.5 * tol[c], 2.0 * inner_delta * rn[c]});
             // GMRES returns the updated residual r - A_low d itself (from its Arnoldi relation)
             // when A_low is its own operator
-            GmresResult r = (o.block && k > 1)
+            GmresResult r = use_block(o, k)
                                 ? bgmres(g, rbuf, g->dd.as<double>(), k, o.precision, o.flags, pre, eps_in, act,
                                          o.itmax - iters, o.restart, s, upd_prec != BIE_FP64 ? rbuf : nullptr,
                                          upd_prec)

@@ -246,9 +246,11 @@ typedef struct {
     int precondition;    /* right diagonal preconditioner 1/t_P (src/solver/multi_rhs.jl:234-247) */
     int check_every;     /* host convergence check period in iterations (default 1) */
     uint32_t flags;      /* BIE_NO_CORRECTIONS etc. applied to the operator */
-    int block;           /* 1: block GMRES for k > 1 (Krylov.block_gmres, src/solver/multi_rhs.jl:285): the
-                            active columns share one block Krylov space (restart = block iterations per
-                            cycle, at most 60); 0: one Arnoldi process per column (default) */
+    int block;           /* 1: block GMRES for 1 < k <= 64 (Krylov.block_gmres, src/solver/multi_rhs.jl:285):
+                            the active columns share one block Krylov space (restart = block iterations
+                            per cycle, at most 60); wider solves run one Arnoldi process per column, which
+                            shares one operator application per iteration over all columns (faster here);
+                            0: one Arnoldi process per column (default) */
 } bie_solve_opts;
 void bie_solve_opts_default(bie_solve_opts* o);
 
