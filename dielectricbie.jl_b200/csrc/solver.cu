@@ -40,7 +40,9 @@ struct bie_geom {
     bie::Buf bv, bq, bvj, bh, bgv, btau, br1, br2, br, bh2, bres, bidx, bflag, xa, ra, binv, bpart, btmp, bwy;
     cublasHandle_t blas = nullptr;  // created on the first block solve
     double* bres_host = nullptr;    // pinned copy of the block residual norms (64 doubles)
-    cudaEvent_t ev_res = nullptr;   // marks that copy in the stream
+    cudaEvent_t ev_res = nullptr;   // marks that copy in the side stream
+    cudaEvent_t ev_h = nullptr;     // marks a new Hessenberg block column in the solver's stream
+    cudaStream_t s_ls = nullptr;    // side stream of the block least-squares updates
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // kernel timing
     struct ProfRec {
@@ -140,15 +142,17 @@ struct Prof {
     int kind;
     cudaStream_t s;
     cudaEvent_t a = nullptr;
+    // timed = false: launches counted but not timed (work overlapped with the solver's stream,
+    // whose event span would include the wait for free SMs)
     Prof(bie_geom* g_, int kind_, cudaStream_t s_, int launches = 1, double pairs = 0, double pair_cols = 0,
-         double bytes = 0)
+         double bytes = 0, bool timed = true)
         : g(g_), kind(kind_), s(s_) {
         bie_kernel_time& t = g->acc[kind];
         t.launches += launches;
         t.pairs += pairs;
         t.pair_cols += pair_cols;
         t.bytes += bytes;
-        if (g->prof_on) {
+        if (g->prof_on && timed) {
             if (g->prof_pending.size() > 8192) prof_drain(g);
             a = pool_event(g);
             BIE_CK(cudaEventRecord(a, s));
@@ -940,6 +944,14 @@ int cholqr2(bie_geom* g, cublasHandle_t h, double* Q, int ka, int64_t n, double*
 // in chunks, 128 columns 98-99 ms against 104-114 ms).
 inline bool use_block(const bie_solve_opts& o, int k) { return o.block && k > 1 && k <= 64; }
 
+// The block solver's side stream, its two events and the pinned residual-norm buffer.
+void ls_init(bie_geom* g) {
+    if (!g->s_ls) BIE_CK(cudaStreamCreateWithFlags(&g->s_ls, cudaStreamNonBlocking));
+    if (!g->ev_h) BIE_CK(cudaEventCreateWithFlags(&g->ev_h, cudaEventDisableTiming));
+    if (!g->ev_res) BIE_CK(cudaEventCreateWithFlags(&g->ev_res, cudaEventDisableTiming));
+    if (!g->bres_host) BIE_CK(cudaMallocHost(&g->bres_host, sizeof(double) * 64));
+}
+
 // One block Krylov space (the method of Krylov.block_gmres, src/solver/multi_rhs.jl:285) for
 // the columns idx (at most 64) of dr. Block Arnoldi with classical Gram-Schmidt against the
 // whole basis (two passes for FP64 solves, one for the reduced-precision inner solves), each
@@ -1054,33 +1066,40 @@ void bgmres_chunk(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
                 pf.add(cholqr2(g, h, Q, ka, n, Hc + rows, (int)L, s, one_pass ? 1 : 2));
                 BIE_CK(cudaMemcpy2DAsync(M + (size_t)(j + 1) * ka, pitchL, Q, pitchK, pitchK, (size_t)n,
                                          cudaMemcpyDeviceToDevice, s));
-                // least squares: the Householder QR of block column j and every column's residual
-                {
-                    double* wy = g->bwy.as<double>();  // each block column's compact-WY form (V, T^T)
-                    if (j > 0) {
-                        const size_t sm = apply_prev_smem(ka);
-                        ensure_smem_limit((const void*)k_bhess_apply_prev, sm);
-                        k_bhess_apply_prev<<<(ka + kApplyCols - 1) / kApplyCols, 256, sm, s>>>(H, (int)L, wy, ka, j);
-                        BIE_CK(cudaGetLastError());
-                        pf.add(1);
-                    }
+            }
+            // Least squares: the Householder QR of block column j and every column's residual,
+            // on the side stream once the column is complete. Only the convergence test needs it:
+            // the next operator application (queued below when convergence is still far) runs
+            // beside it. The two streams touch disjoint data until the cycle's end, where the
+            // solver's stream waits for the side stream (block column j, the right-hand sides,
+            // tau and the WY blocks there; the basis block j + 1, Q and block column j + 1 here).
+            ls_init(g);
+            BIE_CK(cudaEventRecord(g->ev_h, s));
+            BIE_CK(cudaStreamWaitEvent(g->s_ls, g->ev_h, 0));
+            {
+                Prof pf(g, BIE_KERNEL_KRYLOV, g->s_ls, 0, 0, 0, 0, false);
+                double* wy = g->bwy.as<double>();  // each block column's compact-WY form (V, T^T)
+                if (j > 0) {
+                    const size_t sm = apply_prev_smem(ka);
+                    ensure_smem_limit((const void*)k_bhess_apply_prev, sm);
+                    k_bhess_apply_prev<<<(ka + kApplyCols - 1) / kApplyCols, 256, sm, g->s_ls>>>(H, (int)L, wy, ka,
+                                                                                                j);
+                    BIE_CK(cudaGetLastError());
                     pf.add(1);
-                    k_bhess_qr_tile<<<1, 512, 0, s>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
-                                                      g->bres.as<double>(), wy + (size_t)j * wy_stride(ka));
                 }
+                pf.add(1);
+                k_bhess_qr_tile<<<1, 512, 0, g->s_ls>>>(H, (int)L, g->btau.as<double>(), Gv, (int)L, ka, j,
+                                                        g->bres.as<double>(), wy + (size_t)j * wy_stride(ka));
                 BIE_CK(cudaGetLastError());
             }
+            BIE_CK(cudaMemcpyAsync(g->bres_host, g->bres.p, sizeof(double) * ka, cudaMemcpyDeviceToHost, g->s_ls));
+            BIE_CK(cudaEventRecord(g->ev_res, g->s_ls));
             ++it;
             jend = j + 1;
-            // the residual norms to the host. A GMRES iteration lowers a residual by a few times
-            // at most: while the previous one left every column above 16 times its tolerance, the
-            // next iteration will run, and its operator application is queued behind the copy so
-            // that the device works while the host waits for the norms (were the columns to
-            // converge after all, that application is merely unused)
-            if (!g->bres_host) BIE_CK(cudaMallocHost(&g->bres_host, sizeof(double) * 64));
-            if (!g->ev_res) BIE_CK(cudaEventCreateWithFlags(&g->ev_res, cudaEventDisableTiming));
-            BIE_CK(cudaMemcpyAsync(g->bres_host, g->bres.p, sizeof(double) * ka, cudaMemcpyDeviceToHost, s));
-            BIE_CK(cudaEventRecord(g->ev_res, s));
+            // A GMRES iteration lowers a residual by a few times at most: while the previous one
+            // left every column above 16 times its tolerance, the next iteration will run, and its
+            // operator application is queued before the host waits for the norms (were the
+            // columns to converge after all, that application is merely unused)
             if (j > 0 && worst > 16.0 && j + 1 < m && it < itmax) {
                 queue_apply(j + 1);
                 queued = true;
@@ -1098,6 +1117,7 @@ void bgmres_chunk(bie_geom* g, const double* dr, double* dx, int k, int prec, ui
                 break;
             }
         }
+        if (jend > 0) BIE_CK(cudaStreamWaitEvent(s, g->ev_res, 0));  // the cycle's last least-squares update
         // Y = R^-1 Gv[0 : jend ka], x += p .* (V Y)
         {
             Prof pf(g, BIE_KERNEL_KRYLOV, s);  // k_add_rows_scaled (TRSM and DGEMM are cuBLAS's)
@@ -1315,6 +1335,7 @@ bool tuning_read(bie_geom* g, int family, int columns, int pieces, int* nsplit, 
 void geom_trim(bie_geom* g) {
     DeviceGuard dg(g->device);
     BIE_CK(cudaStreamSynchronize(g->stream));
+    if (g->s_ls) BIE_CK(cudaStreamSynchronize(g->s_ls));  // block least-squares work in flight
     bie::Buf* ws[] = {&g->part, &g->bpack, &g->cpart, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn, &g->h, &g->h2,
                       &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid, &g->dpart, &g->rr,
                       &g->xo, &g->dd, &g->io_a, &g->io_b, &g->sol, &g->srcpack, &g->glist, &g->bv, &g->bq,
@@ -1370,6 +1391,7 @@ void geom_destroy(bie_geom* g) {
     {
         DeviceGuard dg(g->device);
         if (g->stream) cudaStreamSynchronize(g->stream);
+        if (g->s_ls) cudaStreamSynchronize(g->s_ls);
         bie::Buf* all[] = {&g->x, &g->y, &g->z, &g->nx, &g->ny, &g->nz, &g->w, &g->diag, &g->pinv, &g->perm, &g->rowptr,
                            &g->col, &g->val, &g->part, &g->small, &g->bpack, &g->errflag, &g->cpart, &g->V, &g->W, &g->R, &g->gv, &g->cs, &g->sn,
                            &g->h, &g->h2, &g->hn, &g->beta, &g->eps, &g->active, &g->jlast, &g->yv, &g->resid,
@@ -1380,6 +1402,8 @@ void geom_destroy(bie_geom* g) {
         if (g->blas) cublasDestroy(g->blas);
         if (g->bres_host) cudaFreeHost(g->bres_host);
         if (g->ev_res) cudaEventDestroy(g->ev_res);
+        if (g->ev_h) cudaEventDestroy(g->ev_h);
+        if (g->s_ls) cudaStreamDestroy(g->s_ls);
         for (auto& r : g->prof_pending) {
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
