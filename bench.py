@@ -332,9 +332,10 @@ def plain_sequential(bie, requests, rtol, restart=200):
 def request_stream(bie, itf, op, wl, precision, device, block=False):
     """Single-point-source requests over three resident geometries (the workload's box and
     two other boxes of 23k-24k nodes, their correction blocks on the device), Poisson
-    arrivals (seeded). An untimed warm-up stream (another seed) goes through a server first,
-    as warm-up steps precede the block solves: it meets the batch widths' first-use costs
-    (launch-shape tuning per kernel instance, workspace growth). The timed stream is served
+    arrivals (seeded). Untimed warm-up first, as warm-up steps precede the block solves: one
+    full-width (128-column) batch per geometry, then a warm-up stream (another seed); they meet
+    the batch widths' first-use costs (launch-shape tuning per kernel instance, workspace
+    growth, graph capture). The timed stream is served
     `repeats` times (the spread of the figures between the runs is reported), then solved
     by the plain FP64 path one request at a time."""
     cnt, rate = SERVE_STREAM["requests"], SERVE_STREAM["rate"]
@@ -355,6 +356,16 @@ def request_stream(bie, itf, op, wl, precision, device, block=False):
             reqs.append((g_op, ("point", [src], eps), float(arr[i])))
         return reqs
 
+    # untimed: a full-width batch (the server's 128 columns) per geometry, so that the widest
+    # kernel instance's tuning and workspace are in place whatever widths the warm-up stream's
+    # timing produces; then the warm-up stream
+    rng_w = np.random.default_rng(wl["seed"] + 98)
+    with bie.SolveServer(max_slots=1, max_batch_rhs=128) as srv:
+        for g_itf, g_op, eps, half in geoms:
+            src = [bie.PointSource(tuple(rng_w.uniform(-half, half)), float(rng_w.standard_normal()))
+                   for _ in range(128)]
+            srv.result(srv.submit_sources(g_op, src, eps, rtol=wl["rtol"], precision=precision, restart=200,
+                                          block=block), sigma=False)
     serve_stream(bie, stream(wl["seed"] + 99), precision, wl["rtol"], block=block)
     reqs = stream(wl["seed"] + 100)
     runs = [serve_stream(bie, reqs, precision, wl["rtol"], block=block) for _ in range(SERVE_STREAM["repeats"])]
