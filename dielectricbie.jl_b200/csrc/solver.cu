@@ -304,17 +304,23 @@ double time_on(bie_geom* g, cudaStream_t s, F&& run) {
 }
 
 // Autotuner: times the candidate launch configurations on the real operand once
-// per (family, columns, pieces) and keeps the fastest; the wave model's choice is
-// kept unless another candidate is more than 2 % faster.
+// per (family, columns, pieces). Among the candidates within 1 % of the fastest it keeps
+// the one with the fewest source splits (the reduction that follows reads one partial per
+// split; near-ties would otherwise be decided by timing noise), then the wave model's
+// choice (the first candidate).
 template <class Launch>
 bie_geom::Tuned tune(bie_geom* g, cudaStream_t s, const std::vector<bie_geom::Tuned>& cands, Launch&& launch) {
     launch(cands.front());  // warm-up (first-use costs)
     std::vector<double> t(cands.size());
     for (size_t i = 0; i < cands.size(); ++i) t[i] = time_on(g, s, [&] { launch(cands[i]); });
-    size_t best = 0;
+    size_t fast = 0;
     for (size_t i = 1; i < cands.size(); ++i)
-        if (t[i] < t[best]) best = i;
-    if (t[best] > 0.98 * t[0]) best = 0;
+        if (t[i] < t[fast]) fast = i;
+    size_t best = fast;
+    for (size_t i = 0; i < cands.size(); ++i)
+        if (t[i] <= 1.01 * t[fast] &&
+            (cands[i].nsplit < cands[best].nsplit || (cands[i].nsplit == cands[best].nsplit && i < best)))
+            best = i;
     bie_geom::Tuned r = cands[best];
     r.ms = t[best];
     return r;
