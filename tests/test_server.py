@@ -191,3 +191,22 @@ def test_server_without_groups_gives_the_same(bie, stream):
         S, st, _ = srv.result(srv.submit_sources(op, srcs, b[5], rtol=1e-10, precision="bf16x3"))
         cnt = srv.counters()
     assert st.solved and np.all(rel_cols(S, ref) < TOL) and cnt["groups"] == 0
+
+
+def test_server_block_request_retry_after_side_stream(bie, stream, monkeypatch):
+    """A block-GMRES request (its least-squares kernels on the geometry's side stream) whose
+    first run meets ENOMEM: the retry releases the workspace (after draining both streams) and
+    runs again, with sigma as the same block solve alone."""
+    ops, reqs = stream
+    rng = np.random.default_rng(7)
+    itf, op, b = ops[0]
+    half = 0.4 * np.array(b[:3])
+    src = [bie.PointSource(tuple(rng.uniform(-half, half)), float(rng.standard_normal())) for _ in range(12)]
+    ref, st_ref = bie.gpu_solve_sources(op, src, b[5], rtol=1e-10, precision="bf16x3", block=True)
+    assert st_ref.solved
+    monkeypatch.setenv("BIE_TEST_SERVER_ENOMEM", "1")
+    with bie.SolveServer(max_slots=1, max_batch_rhs=64) as srv:
+        S, st, _ = srv.result(srv.submit_sources(op, src, b[5], rtol=1e-10, precision="bf16x3", block=True))
+        cnt = srv.counters()
+    assert cnt["enomem_retries"] == 1 and st.solved
+    assert np.all(rel_cols(S, ref) < TOL), rel_cols(S, ref).max()
