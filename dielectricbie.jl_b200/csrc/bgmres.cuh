@@ -16,11 +16,6 @@
 
 namespace bie {
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    return v;
-}
-
 constexpr int kCholThreads = 1024;  // block size of k_chol_inv_smem in the solver
 
 // Cholesky factor R of the k x k Gram matrix G (ld k, upper triangle read) and its inverse,
@@ -281,10 +276,11 @@ __device__ __forceinline__ void tile_reflector(double (&x)[2][16], int t, int k,
 // sides Gv, and every right-hand side's residual. One CTA of 512 threads: column group
 // G = 4 warp + lane / 8 (8 lanes) holds tile column G and right-hand side G in registers,
 // lane g = lane mod 8 the local rows g + 8 r (r < 16). For reflector t the group of column t
-// forms it (LAPACK dlarfg convention: beta = -sign(alpha) mu, tau = (beta - alpha) / beta,
-// tail scaled by 1 / (alpha - beta)) and publishes v through shared
-// memory; after one barrier every group applies it to its columns right of t, over the row
-// slots the reflector meets (tile_reflector; no data-dependent branches).
+// forms it (LAPACK dlarfg convention: mu = |column t from row t on|, beta = mu for alpha <= 0
+// and -mu otherwise, tau = (beta - alpha) / beta, tail scaled by 1 / (alpha - beta)) and
+// publishes v through shared memory; after one barrier every group applies it to its columns
+// right of t, over the row slots the reflector meets (tile_reflector; no data-dependent
+// branches).
 //
 // The block's compact-WY form comes out as well: Q_j = H_0 .. H_{k-1} = I - V T V^T with
 // T = (strictly-upper(V^T V) + diag(1 / tau))^-1 (a zero tau gives a zero row and column of
